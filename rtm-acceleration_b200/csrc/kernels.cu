@@ -1,0 +1,232 @@
+// kernels.cu -- instantiations of the step kernel and the small helper kernels.
+#include <mutex>
+
+#include "kernels.hpp"
+
+namespace rtmb {
+
+static_assert(sizeof(ShotDesc) + 16 <= 512, "ShotDesc must fit the staged descriptor block");
+static_assert(sizeof(ShotDesc) % 4 == 0, "ShotDesc is copied as 32-bit words");
+
+__global__ void advance_counter_kernel(long long* counter, int by) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *counter += by;
+}
+
+namespace {
+
+template <typename T, int H, bool EX, int COLS>
+cudaError_t attr_impl() {
+    using S = TileShape<T, H, kStepWarps, COLS>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(step_kernel<T, H, EX, kStepWarps, COLS>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
+    });
+    return attr_err;
+}
+
+template <typename T, int H, bool EX, int COLS>
+cudaError_t launch_impl(const CUtensorMap& map, const StepParams& p, int grid, cudaStream_t s) {
+    using S = TileShape<T, H, kStepWarps, COLS>;
+    const cudaError_t e = attr_impl<T, H, EX, COLS>();
+    if (e != cudaSuccess) return e;
+    step_kernel<T, H, EX, kStepWarps, COLS><<<grid, kStepThreads, S::SMEM, s>>>(map, p);
+    return cudaGetLastError();
+}
+
+template <typename T, int H, bool EX, int COLS>
+int smem_impl() {
+    return TileShape<T, H, kStepWarps, COLS>::SMEM;
+}
+
+template <typename T, bool EX, int COLS>
+cudaError_t by_half(int half, const CUtensorMap& map, const StepParams& p, int grid, cudaStream_t s) {
+    switch (half) {
+        case 1: return launch_impl<T, 1, EX, COLS>(map, p, grid, s);
+        case 2: return launch_impl<T, 2, EX, COLS>(map, p, grid, s);
+        case 3: return launch_impl<T, 3, EX, COLS>(map, p, grid, s);
+        case 4: return launch_impl<T, 4, EX, COLS>(map, p, grid, s);
+        case 5: return launch_impl<T, 5, EX, COLS>(map, p, grid, s);
+        case 6: return launch_impl<T, 6, EX, COLS>(map, p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T, bool EX, int COLS>
+cudaError_t attr_by_half(int half) {
+    switch (half) {
+        case 1: return attr_impl<T, 1, EX, COLS>();
+        case 2: return attr_impl<T, 2, EX, COLS>();
+        case 3: return attr_impl<T, 3, EX, COLS>();
+        case 4: return attr_impl<T, 4, EX, COLS>();
+        case 5: return attr_impl<T, 5, EX, COLS>();
+        case 6: return attr_impl<T, 6, EX, COLS>();
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t prepare_step(const StepVariant& v) {
+    if (!step_variant_supported(v)) return cudaErrorInvalidValue;
+    if (v.f64) return v.cols == 4 ? attr_by_half<double, false, 4>(v.half) : attr_by_half<double, false, 2>(v.half);
+    if (v.exact) return v.cols == 4 ? attr_by_half<float, true, 4>(v.half) : attr_by_half<float, true, 2>(v.half);
+    return v.cols == 4 ? attr_by_half<float, false, 4>(v.half) : attr_by_half<float, false, 2>(v.half);
+}
+
+bool step_variant_supported(const StepVariant& v) {
+    if (v.half < 1 || v.half > kMaxHalf) return false;
+    if (v.cols != 2 && v.cols != 4) return false;
+    return true;
+}
+
+int step_smem_bytes(const StepVariant& v) {
+    const int elem = v.f64 ? 8 : 4;
+    const int bytes = step_box_z(v) * step_box_x(v) * elem;
+    return 512 + ((bytes + 127) & ~127);
+}
+
+cudaError_t launch_step(const StepVariant& v, const CUtensorMap& map, const StepParams& p, int grid,
+                        cudaStream_t s) {
+    if (!step_variant_supported(v) || grid <= 0) return cudaErrorInvalidValue;
+    if (v.f64) {
+        if (v.cols == 4) return by_half<double, false, 4>(v.half, map, p, grid, s);
+        return by_half<double, false, 2>(v.half, map, p, grid, s);
+    }
+    if (v.exact) {
+        if (v.cols == 4) return by_half<float, true, 4>(v.half, map, p, grid, s);
+        return by_half<float, true, 2>(v.half, map, p, grid, s);
+    }
+    if (v.cols == 4) return by_half<float, false, 4>(v.half, map, p, grid, s);
+    return by_half<float, false, 2>(v.half, map, p, grid, s);
+}
+
+cudaError_t launch_advance_counter(long long* counter, int by, cudaStream_t s) {
+    advance_counter_kernel<<<1, 32, 0, s>>>(counter, by);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- layout moves
+template <typename TS, typename TD>
+__global__ void extract_kernel(const TS* __restrict__ src, int lds, int row0, TD* __restrict__ dst, int nx,
+                               int nz, int count) {
+    const size_t per = (size_t)nx * nz;
+    const size_t total = per * count;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = i / per, r = i % per;
+        const int ix = (int)(r / nz), iz = (int)(r % nz);
+        dst[i] = (TD)src[(k * nx + ix) * (size_t)lds + row0 + iz];
+    }
+}
+
+template <typename T>
+__global__ void insert_kernel(const T* __restrict__ src, int nx, int nz, T* __restrict__ dst, int lds, int row0,
+                              int count) {
+    const size_t per = (size_t)nx * nz;
+    const size_t total = per * count;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = i / per, r = i % per;
+        const int ix = (int)(r / nz), iz = (int)(r % nz);
+        dst[(k * nx + ix) * (size_t)lds + row0 + iz] = src[i];
+    }
+}
+
+static int grid_for(size_t n) {
+    size_t b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)(b > 0 ? b : 1);
+}
+
+cudaError_t launch_extract_f32(const float* src, int lds, int row0, float* dst, int nx, int nz, int count,
+                               cudaStream_t s) {
+    extract_kernel<float, float><<<grid_for((size_t)nx * nz * count), 256, 0, s>>>(src, lds, row0, dst, nx, nz,
+                                                                                   count);
+    return cudaGetLastError();
+}
+cudaError_t launch_extract_f64_to_f32(const double* src, int lds, int row0, float* dst, int nx, int nz,
+                                      cudaStream_t s) {
+    extract_kernel<double, float><<<grid_for((size_t)nx * nz), 256, 0, s>>>(src, lds, row0, dst, nx, nz, 1);
+    return cudaGetLastError();
+}
+cudaError_t launch_extract_f64(const double* src, int lds, int row0, double* dst, int nx, int nz,
+                               cudaStream_t s) {
+    extract_kernel<double, double><<<grid_for((size_t)nx * nz), 256, 0, s>>>(src, lds, row0, dst, nx, nz, 1);
+    return cudaGetLastError();
+}
+cudaError_t launch_insert_f32(const float* src, int nx, int nz, float* dst, int lds, int row0, int count,
+                              cudaStream_t s) {
+    insert_kernel<float><<<grid_for((size_t)nx * nz * count), 256, 0, s>>>(src, nx, nz, dst, lds, row0, count);
+    return cudaGetLastError();
+}
+cudaError_t launch_insert_f64(const double* src, int nx, int nz, double* dst, int lds, int row0, int count,
+                              cudaStream_t s) {
+    insert_kernel<double><<<grid_for((size_t)nx * nz * count), 256, 0, s>>>(src, nx, nz, dst, lds, row0, count);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ FP64 stacking
+// Kahan pairs hold (sum, comp) with the running total = sum - comp.
+__global__ void stack_f32_kernel(const float* __restrict__ I, const float* __restrict__ Ic,
+                                 const float* __restrict__ S, const float* __restrict__ Sc, double* I64, double* S64,
+                                 int nx, int lds, int col0) {
+    const size_t n = (size_t)nx * lds;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t o = (size_t)col0 * lds + i;
+        double vi = (double)I[i], vs = (double)S[i];
+        if (Ic) vi -= (double)Ic[i];
+        if (Sc) vs -= (double)Sc[i];
+        I64[o] += vi;
+        S64[o] += vs;
+    }
+}
+__global__ void stack_f64_kernel(const double* __restrict__ I, const double* __restrict__ S, double* I64,
+                                 double* S64, int nx, int lds, int col0) {
+    const size_t n = (size_t)nx * lds;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t o = (size_t)col0 * lds + i;
+        I64[o] += I[i];
+        S64[o] += S[i];
+    }
+}
+
+cudaError_t launch_stack_f32(const float* I, const float* Ic, const float* S, const float* Sc, double* I64,
+                             double* S64, int nx, int lds, int col0, cudaStream_t s) {
+    stack_f32_kernel<<<grid_for((size_t)nx * lds), 256, 0, s>>>(I, Ic, S, Sc, I64, S64, nx, lds, col0);
+    return cudaGetLastError();
+}
+cudaError_t launch_stack_f64(const double* I, const double* S, double* I64, double* S64, int nx, int lds,
+                             int col0, cudaStream_t s) {
+    stack_f64_kernel<<<grid_for((size_t)nx * lds), 256, 0, s>>>(I, S, I64, S64, nx, lds, col0);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ single-step imaging
+__global__ void imaging_dense_kernel(const float* __restrict__ fwd, const float* __restrict__ bwd, float* I,
+                                     float* S, int nx, int nz, int nb, int nze) {
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        const float f = fwd[i];
+        const float b = bwd[(size_t)(ix + nb) * nze + nb + iz];
+        I[i] = __fadd_rn(I[i], __fmul_rn(f, b));
+        S[i] = __fadd_rn(S[i], __fmul_rn(f, f));
+    }
+}
+
+cudaError_t launch_imaging_dense(const float* fwd, const float* bwd_ext, float* I, float* S, int nx, int nz,
+                                 int nb, int nze, cudaStream_t s) {
+    imaging_dense_kernel<<<grid_for((size_t)nx * nz), 256, 0, s>>>(fwd, bwd_ext, I, S, nx, nz, nb, nze);
+    return cudaGetLastError();
+}
+
+__global__ void widen_kernel(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+cudaError_t launch_widen(const float* src, double* dst, size_t n, cudaStream_t s) {
+    widen_kernel<<<grid_for(n), 256, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+}  // namespace rtmb

@@ -1,0 +1,64 @@
+// kernels.hpp -- host-callable launchers for librtm_b200's device code.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "internal.hpp"
+#include "step_kernel.cuh"
+
+namespace rtmb {
+
+// Compile-time variant of the step kernel, chosen at run time.
+struct StepVariant {
+    bool f64 = false;   // double fields (the FP64 run)
+    int half = 4;       // order / 2
+    bool exact = true;  // IEEE unfused float arithmetic (bit-identical path)
+    int cols = 4;       // columns per warp; tile is 128 rows x (8*cols) columns
+};
+
+constexpr int kStepWarps = 8;
+constexpr int kStepThreads = kStepWarps * 32;
+
+inline int step_tile_x(const StepVariant& v) { return kStepWarps * v.cols; }
+inline int step_halo_rows(const StepVariant& v) { return (v.half + 3) & ~3; }
+inline int step_box_z(const StepVariant& v) { return kTileZ + 2 * step_halo_rows(v); }
+inline int step_box_x(const StepVariant& v) { return step_tile_x(v) + 2 * v.half; }
+int step_smem_bytes(const StepVariant& v);
+bool step_variant_supported(const StepVariant& v);
+
+// Sets the kernel's shared-memory attribute (call before any stream capture).
+cudaError_t prepare_step(const StepVariant& v);
+
+// Launch one time step over `grid` tiles.
+cudaError_t launch_step(const StepVariant& v, const CUtensorMap& map, const StepParams& p, int grid,
+                        cudaStream_t s);
+
+cudaError_t launch_advance_counter(long long* counter, int by, cudaStream_t s);
+
+// dst[ix*nz+iz] = src[ix*lds + row0 + iz]   (padded image/snapshot -> dense)
+cudaError_t launch_extract_f32(const float* src, int lds, int row0, float* dst, int nx, int nz, int count,
+                               cudaStream_t s);
+cudaError_t launch_extract_f64_to_f32(const double* src, int lds, int row0, float* dst, int nx, int nz,
+                                      cudaStream_t s);
+cudaError_t launch_extract_f64(const double* src, int lds, int row0, double* dst, int nx, int nz, cudaStream_t s);
+// dense -> padded for `count` consecutive snapshots (host snapshots uploaded for backward)
+cudaError_t launch_insert_f32(const float* src, int nx, int nz, float* dst, int lds, int row0, int count,
+                              cudaStream_t s);
+cudaError_t launch_insert_f64(const double* src, int nx, int nz, double* dst, int lds, int row0, int count,
+                              cudaStream_t s);
+
+// FP64 cross-shot stack of one shot's image/illumination, shot columns placed
+// at model column `col0`.  comp arrays may be null (uncompensated sums).
+cudaError_t launch_stack_f32(const float* I, const float* Ic, const float* S, const float* Sc, double* I64,
+                             double* S64, int nx, int lds, int col0, cudaStream_t s);
+cudaError_t launch_stack_f64(const double* I, const double* S, double* I64, double* S64, int nx, int lds,
+                             int col0, cudaStream_t s);
+
+// One zero-lag imaging step on dense arrays (reference imaging.cpp:25-40).
+cudaError_t launch_imaging_dense(const float* fwd, const float* bwd_ext, float* I, float* S, int nx, int nz,
+                                 int nb, int nze, cudaStream_t s);
+
+// float -> double widening of a dense array.
+cudaError_t launch_widen(const float* src, double* dst, size_t n, cudaStream_t s);
+
+}  // namespace rtmb
