@@ -89,7 +89,7 @@ int Engine::init() {
     RTMB_CUDA(cudaMemsetAsync(counter_.get(), 0, sizeof(long long), stream_));
     RTMB_CUDA(cudaMemsetAsync(errword_.get(), 0, sizeof(int), stream_));
     RTMB_CUDA(cudaStreamSynchronize(stream_));
-    cols_ = cfg_.tile_cols == 16 ? 2 : 4;
+    cols_ = cfg_.tile_cols == 32 ? 4 : 2;
     inited_ = true;
     return RTM_B200_OK;
 }
@@ -219,12 +219,13 @@ int Engine::copy_shots(Model& m, const rtm_b200_shot* shots, int nshots, bool ne
 }
 
 // -------------------------------------------------------------- pool, slots
-int Engine::encode_map(int half, CUtensorMap* out) {
+int Engine::encode_map(int half, bool with_halo, CUtensorMap* out) {
     StepVariant v;
     v.f64 = f64_; v.half = half; v.cols = cols_;
-    const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)nslots_ * 2};
+    const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)nslots_ * kFieldBuffers};
     const cuuint64_t strides[2] = {(cuuint64_t)ldz_cap_ * elem(), (cuuint64_t)ldz_cap_ * nxe_cap_ * elem()};
-    const cuuint32_t box[3] = {(cuuint32_t)step_box_z(v), (cuuint32_t)step_box_x(v), 1};
+    const cuuint32_t box[3] = {(cuuint32_t)(with_halo ? step_box_z(v) : kTileZ),
+                               (cuuint32_t)(with_halo ? step_box_x(v) : step_tile_x(v)), 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = tensor_map_encoder()(
         out, f64_ ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, pool_.get(), dims, strides,
@@ -244,7 +245,7 @@ int Engine::ensure_pool(int nslots, int nxe_cap, int ldz_cap) {
     nslots_ = std::max(nslots, nslots_);
     nxe_cap_ = std::max(nxe_cap, nxe_cap_);
     ldz_cap_ = ldz_cap;
-    const size_t bytes = (size_t)nslots_ * 2 * nxe_cap_ * ldz_cap_ * elem();
+    const size_t bytes = (size_t)nslots_ * kFieldBuffers * nxe_cap_ * ldz_cap_ * elem();
     cudaError_t e = pool_.alloc(bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -310,6 +311,14 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                      geo.nclamped, sh.nrec + 1, (gs.nx - 1) * m->dx, (gs.nz - 1) * m->dz);
     RTMB_TRY(ensure_slot(s, *m, sh, gs, modelling));
     Slot& sl = slots_[(size_t)s];
+    // Which tiles hold receiver cells (the kernel only walks receiver lists there).
+    const int TX = kStepWarps * cols_;
+    const int ntx = (gs.nxe + TX - 1) / TX;
+    std::vector<uint8_t> tflags((size_t)ntx * gs.ntz, 0);
+    for (int x = 0; x < gs.nxe; ++x)
+        for (int j = geo.col_start[(size_t)x]; j < geo.col_start[(size_t)x + 1]; ++j)
+            tflags[(size_t)(x / TX) * gs.ntz + geo.pts[(size_t)j].z / kTileZ] = 1;
+    RTMB_CUDA(sl.tile_pts.reserve(tflags.size()));
 
     // Stage everything this job uploads in the slot's pinned buffer.
     std::vector<float> wx((size_t)gs.nxe);
@@ -322,6 +331,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     const size_t o_pts = take(geo.pts.size() * sizeof(PointEntry));
     const size_t o_ir = take(geo.ir.size() * 4);
     const size_t o_desc = take(sizeof(ShotDesc));
+    const size_t o_tf = take(tflags.size());
     const size_t o_tr = take(trace_elems * 4);
     RTMB_CUDA(cudaEventSynchronize(sl.staged));   // previous upload from this buffer is done
     if (cudaSuccess != sl.stage.reserve(off)) {
@@ -334,12 +344,13 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     if (!geo.pts.empty()) std::memcpy(st + o_pts, geo.pts.data(), geo.pts.size() * sizeof(PointEntry));
     if (!geo.ir.empty()) std::memcpy(st + o_ir, geo.ir.data(), geo.ir.size() * 4);
     if (trace_elems) std::memcpy(st + o_tr, sh.traces, trace_elems * 4);
+    std::memcpy(st + o_tf, tflags.data(), tflags.size());
 
     // Descriptor.
     ShotDesc d{};
     d.nxe = gs.nxe; d.nze = gs.nze; d.nx = gs.nx; d.nz = gs.nz; d.nb = gs.nb;
     d.model_x0 = sh.x0; d.win_nx = gs.nx;
-    d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz;
+    d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz; d.ntx = ntx;
     d.nt = m->nt; d.si = m->si; d.nsnap = m->nsnap;
     job.first_phase_step = backward_only == 1 ? m->nt : 0;
     job.g0 = g_ - job.first_phase_step;
@@ -360,6 +371,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     d.wavelet = m->wavelet.get<float>();
     d.traces = sl.traces.get<float>();
     d.col_start = sl.col_start.get<int>();
+    d.tile_pts = sl.tile_pts.get<uint8_t>();
     d.pts = sl.pts.get<PointEntry>();
     d.pts_ir = sl.ir.get<int>();
     d.rec_out = sl.rec.get<float>();
@@ -405,8 +417,16 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
         RTMB_CUDA(cudaMemcpyAsync(sl.ir.get(), st + o_ir, geo.ir.size() * 4, cudaMemcpyHostToDevice, stream_));
     if (trace_elems)
         RTMB_CUDA(cudaMemcpyAsync(sl.traces.get(), st + o_tr, trace_elems * 4, cudaMemcpyHostToDevice, stream_));
+    RTMB_CUDA(cudaMemcpyAsync(sl.tile_pts.get(), st + o_tf, tflags.size(), cudaMemcpyHostToDevice, stream_));
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
+    // The slot's (v dt)^2 on the shot's extended grid (third field buffer).
+    {
+        char* vbuf = pool_.get<char>() + ((size_t)s * kFieldBuffers + 2) * nxe_cap_ * ldz_cap_ * elem();
+        RTMB_CUDA(launch_slot_vdt2(vbuf, f64_, ldz_cap_, gs.nxe, m->vdt2.get<float>(), m->g.ldz, gs.nb, gs.nx,
+                                   sh.x0, stream_));
+        launches_ += 1;
+    }
     RTMB_CUDA(cudaEventRecord(sl.staged, stream_));
 
     job.active = true;
@@ -495,8 +515,9 @@ int Engine::build_tiles() {
     RTMB_CUDA(cudaMemcpy(tiles_.get(), all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     for (auto& g : groups_) {
         if (!maps_.count(g.half)) {
-            CUtensorMap mp;
-            RTMB_TRY(encode_map(g.half, &mp));
+            MapPair mp;
+            RTMB_TRY(encode_map(g.half, true, &mp.pc));
+            RTMB_TRY(encode_map(g.half, false, &mp.box));
             maps_[g.half] = mp;
         }
         StepVariant v;
@@ -537,7 +558,7 @@ int Engine::run_chunk(int steps) {
                 StepParams p{};
                 p.fields = pool_.get();
                 p.buf_stride = (long long)nxe_cap_ * ldz_cap_;
-                p.slot_stride = 2 * p.buf_stride;
+                p.slot_stride = kFieldBuffers * p.buf_stride;
                 p.ldz = ldz_cap_;
                 p.ntiles = g.count;
                 p.descs = descs_.get<ShotDesc>();
@@ -545,7 +566,8 @@ int Engine::run_chunk(int steps) {
                 p.step_counter = counter_.get<long long>();
                 p.step_offset = j;
                 p.error_word = errword_.get<int>();
-                RTMB_CUDA(launch_step(v, maps_[g.half], p, g.count, stream_));
+                const MapPair& mp = maps_[g.half];
+                RTMB_CUDA(launch_step(v, mp.pc, mp.box, p, stream_));
             }
         RTMB_CUDA(launch_advance_counter(counter_.get<long long>(), steps, stream_));
         return RTM_B200_OK;

@@ -81,7 +81,7 @@ struct Job {
 };
 
 struct Slot {
-    DevMem wx, col_start, pts, ir, traces, rec, acc;
+    DevMem wx, col_start, pts, ir, traces, rec, acc, tile_pts;
     PinnedMem stage;
     cudaEvent_t staged = nullptr;      // H2D from `stage` finished
 };
@@ -130,7 +130,7 @@ private:
     // pool / slots
     int ensure_pool(int nslots, int nxe_cap, int ldz_cap);
     int ensure_slot(int s, const Model& m, const ShotData& sh, const GridDims& gs, bool modelling);
-    int encode_map(int half, CUtensorMap* out);
+    int encode_map(int half, bool with_halo, CUtensorMap* out);
 
     // scheduling
     int start_job(int slot, Model* m, int shot, bool modelling, float* rec_host, int backward_only,
@@ -166,10 +166,11 @@ private:
 
     std::unique_ptr<Model> model_;           // the setup() model
 
-    // field pool: T[nslots][2][nxe_cap][ldz_cap]
+    // field pool: T[nslots][3][nxe_cap][ldz_cap]
     DevMem pool_;
     int nslots_ = 0, nxe_cap_ = 0, ldz_cap_ = 0;
-    std::map<int, CUtensorMap> maps_;        // by half
+    struct MapPair { CUtensorMap pc, box; };
+    std::map<int, MapPair> maps_;            // by half: p^n box with halo; 128 x TX box
     std::vector<Slot> slots_;
     std::vector<Job> jobs_;
     DevMem descs_;                           // ShotDesc[nslots]

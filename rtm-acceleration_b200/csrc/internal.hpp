@@ -4,15 +4,16 @@
 // Device layout (every array is "zfast", depth contiguous, like the reference's
 // index = ix*nz + iz, include/rtm_types.hpp:10-15 of the reference):
 //
-//   field pool   T[nslot][2][NXE][LDZ]  two time levels per shot slot (the
-//                leapfrog runs in place: p^{n+1} overwrites p^{n-1}); a shot's
-//                extended grid (nxe x nze) sits in the top-left corner of its
-//                slot.  LDZ is a multiple of 4 so every column starts on a
-//                16-byte boundary (float4 / TMA alignment).
+//   field pool   T[nslot][3][NXE][LDZ]  per shot slot: two time levels (the
+//                leapfrog runs in place: p^{n+1} overwrites p^{n-1}) and the
+//                shot's (v dt)^2 on its extended grid; a shot's extended grid
+//                (nxe x nze) sits in the top-left corner of its slot.  LDZ is a
+//                multiple of 8 so every column starts on a 32-byte boundary.
 //   vdt2 model   float[model_nx][LDZ]  (v dt)^2 for every interior model column,
-//                already extended in depth by edge replication; the extension in
-//                x is done by clamping the column index inside the kernel, which
-//                also gives each aperture window its own edge replication.
+//                extended in depth by edge replication; a shot's slot copy is
+//                extended in x by clamping to its aperture window, which gives
+//                each window its own edge replication (reference
+//                src/rtm/rtm_cpu.cpp:33-42 on the cropped model).
 //   snapshots    S[nsnap][nx][lds]  interior columns, rows [zs0, zs0+lds) of the
 //                extended grid (zs0 = nb rounded down to 4, lds multiple of 4).
 //   image/illum  A[nx][lds]          same layout as one snapshot.
@@ -53,6 +54,7 @@ struct ShotDesc {
     int win_nx;          // window width in model columns (== nx)
     int zs0, lds;        // snapshot/image row origin (extended z) and pitch
     int ntz;             // tiles in z (scale-exponent stride)
+    int ntx;             // tiles in x
     // time
     int nt, si, nsnap;
     long long g0;        // global step at which forward step 0 runs
@@ -75,6 +77,7 @@ struct ShotDesc {
     const float* wavelet;    // nt
     const float* traces;     // nrec * trace_nt, trace-major
     const int* col_start;    // nxe+1 offsets into pts
+    const uint8_t* tile_pts; // ntx*ntz flags: tile holds receiver cells
     const PointEntry* pts;
     const int* pts_ir;
     float* rec_out;          // nrec * nt trace-major (modelling)
@@ -85,6 +88,8 @@ struct ShotDesc {
     void* img_c;             // compensation words (kAccCompensated)
     void* ill_c;
 };
+
+constexpr int kFieldBuffers = 3;     // p^n / p^{n+1}, p^{n-1}, (v dt)^2
 
 // One CTA's work item.
 struct TileRef {

@@ -27,11 +27,32 @@ cudaError_t attr_impl() {
 }
 
 template <typename T, int H, bool EX, int COLS>
-cudaError_t launch_impl(const CUtensorMap& map, const StepParams& p, int grid, cudaStream_t s) {
+int max_grid_impl() {
+    using S = TileShape<T, H, kStepWarps, COLS>;
+    static std::once_flag once;
+    static int grid = 0;
+    std::call_once(once, [] {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (attr_impl<T, H, EX, COLS>() == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_kernel<T, H, EX, kStepWarps, COLS>,
+                                                          kStepThreads, S::SMEM) == cudaSuccess)
+            grid = sms * (per > 0 ? per : 1);
+        else
+            grid = sms > 0 ? sms : 148;
+    });
+    return grid;
+}
+
+template <typename T, int H, bool EX, int COLS>
+cudaError_t launch_impl(const CUtensorMap& mpc, const CUtensorMap& mpp, const StepParams& p, cudaStream_t s) {
     using S = TileShape<T, H, kStepWarps, COLS>;
     const cudaError_t e = attr_impl<T, H, EX, COLS>();
     if (e != cudaSuccess) return e;
-    step_kernel<T, H, EX, kStepWarps, COLS><<<grid, kStepThreads, S::SMEM, s>>>(map, p);
+    const int cap = max_grid_impl<T, H, EX, COLS>();
+    const int grid = p.ntiles < cap ? p.ntiles : cap;
+    step_kernel<T, H, EX, kStepWarps, COLS><<<grid, kStepThreads, S::SMEM, s>>>(mpc, mpp, p);
     return cudaGetLastError();
 }
 
@@ -41,15 +62,28 @@ int smem_impl() {
 }
 
 template <typename T, bool EX, int COLS>
-cudaError_t by_half(int half, const CUtensorMap& map, const StepParams& p, int grid, cudaStream_t s) {
+cudaError_t by_half(int half, const CUtensorMap& a, const CUtensorMap& b, const StepParams& p, cudaStream_t s) {
     switch (half) {
-        case 1: return launch_impl<T, 1, EX, COLS>(map, p, grid, s);
-        case 2: return launch_impl<T, 2, EX, COLS>(map, p, grid, s);
-        case 3: return launch_impl<T, 3, EX, COLS>(map, p, grid, s);
-        case 4: return launch_impl<T, 4, EX, COLS>(map, p, grid, s);
-        case 5: return launch_impl<T, 5, EX, COLS>(map, p, grid, s);
-        case 6: return launch_impl<T, 6, EX, COLS>(map, p, grid, s);
+        case 1: return launch_impl<T, 1, EX, COLS>(a, b, p, s);
+        case 2: return launch_impl<T, 2, EX, COLS>(a, b, p, s);
+        case 3: return launch_impl<T, 3, EX, COLS>(a, b, p, s);
+        case 4: return launch_impl<T, 4, EX, COLS>(a, b, p, s);
+        case 5: return launch_impl<T, 5, EX, COLS>(a, b, p, s);
+        case 6: return launch_impl<T, 6, EX, COLS>(a, b, p, s);
         default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T, bool EX, int COLS>
+int grid_by_half(int half) {
+    switch (half) {
+        case 1: return max_grid_impl<T, 1, EX, COLS>();
+        case 2: return max_grid_impl<T, 2, EX, COLS>();
+        case 3: return max_grid_impl<T, 3, EX, COLS>();
+        case 4: return max_grid_impl<T, 4, EX, COLS>();
+        case 5: return max_grid_impl<T, 5, EX, COLS>();
+        case 6: return max_grid_impl<T, 6, EX, COLS>();
+        default: return 0;
     }
 }
 
@@ -70,6 +104,7 @@ cudaError_t attr_by_half(int half) {
 
 cudaError_t prepare_step(const StepVariant& v) {
     if (!step_variant_supported(v)) return cudaErrorInvalidValue;
+    if (step_max_grid(v) <= 0) return cudaErrorInvalidValue;
     if (v.f64) return v.cols == 4 ? attr_by_half<double, false, 4>(v.half) : attr_by_half<double, false, 2>(v.half);
     if (v.exact) return v.cols == 4 ? attr_by_half<float, true, 4>(v.half) : attr_by_half<float, true, 2>(v.half);
     return v.cols == 4 ? attr_by_half<float, false, 4>(v.half) : attr_by_half<float, false, 2>(v.half);
@@ -83,23 +118,31 @@ bool step_variant_supported(const StepVariant& v) {
 
 int step_smem_bytes(const StepVariant& v) {
     const int elem = v.f64 ? 8 : 4;
-    const int bytes = step_box_z(v) * step_box_x(v) * elem;
-    return 512 + ((bytes + 127) & ~127);
+    const int pc = step_box_z(v) * step_box_x(v) * elem;
+    const int box = kTileZ * step_tile_x(v) * elem;
+    return 2 * (1408 + ((pc + 127) & ~127) + 2 * ((box + 127) & ~127));
 }
 
-cudaError_t launch_step(const StepVariant& v, const CUtensorMap& map, const StepParams& p, int grid,
+int step_max_grid(const StepVariant& v) {
+    if (!step_variant_supported(v)) return 0;
+    if (v.f64) return v.cols == 4 ? grid_by_half<double, false, 4>(v.half) : grid_by_half<double, false, 2>(v.half);
+    if (v.exact) return v.cols == 4 ? grid_by_half<float, true, 4>(v.half) : grid_by_half<float, true, 2>(v.half);
+    return v.cols == 4 ? grid_by_half<float, false, 4>(v.half) : grid_by_half<float, false, 2>(v.half);
+}
+
+cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUtensorMap& mpp, const StepParams& p,
                         cudaStream_t s) {
-    if (!step_variant_supported(v) || grid <= 0) return cudaErrorInvalidValue;
+    if (!step_variant_supported(v) || p.ntiles <= 0) return cudaErrorInvalidValue;
     if (v.f64) {
-        if (v.cols == 4) return by_half<double, false, 4>(v.half, map, p, grid, s);
-        return by_half<double, false, 2>(v.half, map, p, grid, s);
+        if (v.cols == 4) return by_half<double, false, 4>(v.half, mpc, mpp, p, s);
+        return by_half<double, false, 2>(v.half, mpc, mpp, p, s);
     }
     if (v.exact) {
-        if (v.cols == 4) return by_half<float, true, 4>(v.half, map, p, grid, s);
-        return by_half<float, true, 2>(v.half, map, p, grid, s);
+        if (v.cols == 4) return by_half<float, true, 4>(v.half, mpc, mpp, p, s);
+        return by_half<float, true, 2>(v.half, mpc, mpp, p, s);
     }
-    if (v.cols == 4) return by_half<float, false, 4>(v.half, map, p, grid, s);
-    return by_half<float, false, 2>(v.half, map, p, grid, s);
+    if (v.cols == 4) return by_half<float, false, 4>(v.half, mpc, mpp, p, s);
+    return by_half<float, false, 2>(v.half, mpc, mpp, p, s);
 }
 
 cudaError_t launch_advance_counter(long long* counter, int by, cudaStream_t s) {
@@ -217,6 +260,28 @@ __global__ void imaging_dense_kernel(const float* __restrict__ fwd, const float*
 cudaError_t launch_imaging_dense(const float* fwd, const float* bwd_ext, float* I, float* S, int nx, int nz,
                                  int nb, int nze, cudaStream_t s) {
     imaging_dense_kernel<<<grid_for((size_t)nx * nz), 256, 0, s>>>(fwd, bwd_ext, I, S, nx, nz, nb, nze);
+    return cudaGetLastError();
+}
+
+template <typename T>
+__global__ void slot_vdt2_kernel(T* __restrict__ dst, int ldz, int nxe, const float* __restrict__ model,
+                                 int ldz_model, int nb, int win_nx, int x0) {
+    const size_t n = (size_t)nxe * ldz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i / ldz), z = (int)(i % ldz);
+        int mx = x - nb;
+        mx = mx < 0 ? 0 : (mx > win_nx - 1 ? win_nx - 1 : mx);
+        dst[i] = z < ldz_model ? (T)model[(size_t)(mx + x0) * ldz_model + z] : (T)0;
+    }
+}
+
+cudaError_t launch_slot_vdt2(void* dst, bool f64, int ldz, int nxe, const float* model, int ldz_model, int nb,
+                             int win_nx, int x0, cudaStream_t s) {
+    const int g = grid_for((size_t)nxe * ldz);
+    if (f64)
+        slot_vdt2_kernel<double><<<g, 256, 0, s>>>((double*)dst, ldz, nxe, model, ldz_model, nb, win_nx, x0);
+    else
+        slot_vdt2_kernel<float><<<g, 256, 0, s>>>((float*)dst, ldz, nxe, model, ldz_model, nb, win_nx, x0);
     return cudaGetLastError();
 }
 

@@ -29,9 +29,19 @@ bool step_variant_supported(const StepVariant& v);
 // Sets the kernel's shared-memory attribute (call before any stream capture).
 cudaError_t prepare_step(const StepVariant& v);
 
-// Launch one time step over `grid` tiles.
-cudaError_t launch_step(const StepVariant& v, const CUtensorMap& map, const StepParams& p, int grid,
-                        cudaStream_t s);
+// Resident CTAs of the persistent step kernel on this device (grid cap).
+int step_max_grid(const StepVariant& v);
+
+// Launch one time step over p.ntiles tiles (grid = min(ntiles, resident CTAs)).
+// map_pc: box of p^n with halo (step_box_z x step_box_x); map_box: box of
+// 128 x step_tile_x (p^{n-1} and (v dt)^2).  Both describe the field pool.
+cudaError_t launch_step(const StepVariant& v, const CUtensorMap& map_pc, const CUtensorMap& map_box,
+                        const StepParams& p, cudaStream_t s);
+
+// Fill a slot's (v dt)^2 buffer (nxe columns x ldz rows) from the model table,
+// columns clamped to the aperture window [x0, x0+win_nx).
+cudaError_t launch_slot_vdt2(void* dst, bool f64, int ldz, int nxe, const float* model, int ldz_model, int nb,
+                             int win_nx, int x0, cudaStream_t s);
 
 cudaError_t launch_advance_counter(long long* counter, int by, cudaStream_t s);
 

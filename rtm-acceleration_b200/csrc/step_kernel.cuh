@@ -160,136 +160,200 @@ struct Halo {
     static constexpr int HP = (H + 3) & ~3;
 };
 
+// Shared-memory stage of the pipelined step kernel:
+//   [0, 8)        mbarrier of this stage's TMA loads
+//   [16, 64)      TileInfo: what the tile does this step (written by warp 0)
+//   [64, ...)     the tile's ShotDesc
+//   [WX_OFF, ..)  taper weights wx of the tile's TX columns
+//   [WZ_OFF, ..)  taper weights wz of the tile's 128 rows
+//   [CS_OFF, ..)  receiver-list offsets col_start[x0 .. x0+TX] (receiver tiles)
+//   [PC_OFF, ..)  TMA box of p^n with the stencil halo      (SZ x SX)
+//   [PP_OFF, ..)  TMA box of p^{n-1}                         (128 x TX)
+//   [VD_OFF, ..)  TMA box of the shot's (v dt)^2             (128 x TX)
+struct TileInfo {
+    int active, fwd, first, it, cur, x0, z0, tz;
+    int do_snap, do_image, ksnap, has_pts;
+};
+
 template <typename T, int H, int NWARP, int COLS>
 struct TileShape {
     static constexpr int HP = Halo<H>::HP;
     static constexpr int TX = NWARP * COLS;
-    static constexpr int SZ = kTileZ + 2 * HP;   // rows held in shared memory
-    static constexpr int SX = TX + 2 * H;        // columns held in shared memory
-    static constexpr int BYTES = SZ * SX * (int)sizeof(T);
-    static constexpr int DESC_BYTES = 512;                      // barrier + staged ShotDesc
-    static constexpr int SMEM = DESC_BYTES + ((BYTES + 127) & ~127);
+    static constexpr int SZ = kTileZ + 2 * HP;   // rows of the p^n box
+    static constexpr int SX = TX + 2 * H;        // columns of the p^n box
+    static constexpr int PC_BYTES = SZ * SX * (int)sizeof(T);
+    static constexpr int BOX_BYTES = kTileZ * TX * (int)sizeof(T);
+    static constexpr int INFO_OFF = 16;
+    static constexpr int DESC_OFF = 64;
+    static constexpr int WX_OFF = 512;
+    static constexpr int WZ_OFF = WX_OFF + 128;
+    static constexpr int CS_OFF = WZ_OFF + kTileZ * 4;
+    static constexpr int HDR = 1408;
+    static constexpr int PC_OFF = HDR;
+    static constexpr int PP_OFF = PC_OFF + ((PC_BYTES + 127) & ~127);
+    static constexpr int VD_OFF = PP_OFF + ((BOX_BYTES + 127) & ~127);
+    static constexpr int STAGE = VD_OFF + ((BOX_BYTES + 127) & ~127);
+    static constexpr int SMEM = 2 * STAGE;
+    static_assert(TX <= 32, "wx staging holds at most 32 columns");
+    static_assert(CS_OFF + 4 * (TX + 1) <= HDR, "stage header overflow");
+    static_assert(INFO_OFF + sizeof(TileInfo) <= DESC_OFF, "tile info overflows its block");
+    static_assert(DESC_OFF + sizeof(ShotDesc) <= WX_OFF, "descriptor overflows its block");
 };
 
-// ------------------------------------------------------------- the tile
-// Computes one tile after its p^n box has landed in shared memory.
-template <typename T, int H, bool EXACT, int NWARP, int COLS>
-__device__ __forceinline__ void compute_tile(const ShotDesc& d, const T* __restrict__ sm, T* __restrict__ pcur,
-                                             T* __restrict__ pnext, int ldz, int x0, int z0, int tz, int it,
-                                             bool fwd, bool first) {
-    using A = Arith<T, EXACT>;
-    using S = TileShape<T, H, NWARP, COLS>;
-    constexpr int HP = S::HP;
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int zr = z0 + 4 * lane;                // first of this thread's 4 rows
-    const bool lane_in = zr < d.nze;
-    const int nxe = d.nxe, nze = d.nze;
-
-    const T c0 = (T)d.c0;
-    T cx[H + 1], cz[H + 1];
-#pragma unroll
-    for (int k = 1; k <= H; ++k) { cx[k] = (T)d.cx[k]; cz[k] = (T)d.cz[k]; }
-
-    // Row masks: rows inside [H, nze-H) are updated, the outer H-ring stays 0.
-    bool row_ok[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) row_ok[q] = (zr + q >= H) && (zr + q < nze - H);
-
-    float wzv[4] = {0.f, 0.f, 0.f, 0.f};
-    if (lane_in) ldg4(d.wz + zr, wzv);
-
-    const bool store_step = (it % d.si) == 0;
-    const bool do_snap = fwd && store_step && (d.flags & kFlagSnapshots);
-    const bool do_image = !fwd && store_step && (d.flags & kFlagImage);
-    const int ksnap = it / d.si;
-    const bool lane_snap = lane_in && zr >= d.zs0 && zr < d.zs0 + d.lds;
-
-#pragma unroll 1
-    for (int c = 0; c < COLS; ++c) {
-        const int x = x0 + warp * COLS + c;
-        if (x >= nxe) break;                     // warp-uniform
-        const int sx = x - x0 + H;               // column inside the smem tile
-        const T* col = sm + (size_t)sx * S::SZ + 4 * lane + HP;   // row zr in smem
-
-        // p^{n-1} (own cells), vdt2 (model column clamped to the window), taper
-        T pp[4] = {0, 0, 0, 0};
-        float vd[4] = {0.f, 0.f, 0.f, 0.f};
-        T* pn_col = pnext + (size_t)x * ldz;
-        if (lane_in) {
-            if (!first) ld4(pn_col + zr, pp);
-            int mx = x - d.nb;
-            mx = mx < 0 ? 0 : (mx > d.win_nx - 1 ? d.win_nx - 1 : mx);
-            ldg4(d.vdt2 + (size_t)(mx + d.model_x0) * d.ldz_model + zr, vd);
+// Decodes a snapshot value group (4 rows).
+template <typename T>
+__device__ __forceinline__ void load_snapshot4(const ShotDesc& d, size_t cell, size_t eidx, T (&f)[4]) {
+    if (d.snap_type == kSnapF32 || d.snap_type == kSnapF64) {
+        ld4cs(reinterpret_cast<const T*>(d.snap) + cell, f);
+    } else {
+        const uint2 packed =
+            __ldcs(reinterpret_cast<const uint2*>(reinterpret_cast<const uint16_t*>(d.snap) + cell));
+        const float sc = pow2f((int)__ldg(d.snap_exp + eidx));
+        float2 a, b;
+        if (d.snap_type == kSnapF16) {
+            a = __half22float2(*reinterpret_cast<const __half2*>(&packed.x));
+            b = __half22float2(*reinterpret_cast<const __half2*>(&packed.y));
+        } else {
+            a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&packed.x));
+            b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&packed.y));
         }
-        const float wxv = __ldg(d.wx + x);
+        f[0] = (T)(a.x * sc); f[1] = (T)(a.y * sc); f[2] = (T)(b.x * sc); f[3] = (T)(b.y * sc);
+    }
+}
 
-        // Laplacian from shared memory (zero on the first step of a pass).
+// ------------------------------------------------------ column arithmetic
+// One column of 4 rows: Laplacian from the p^n box, leapfrog with the sponge,
+// before injection and masking.  Generic scalar form (used for double).
+template <typename T, int H, bool EXACT, int SZ, int HP>
+struct ColumnMath {
+    static __device__ __forceinline__ void run(const T* col, const T (&pp)[4], const T (&vd)[4], float wxv,
+                                               const float (&wz)[4], T c0, const float* cx, const float* cz,
+                                               bool first, T (&val)[4]) {
+        using A = Arith<T, EXACT>;
         T zz[4 + 2 * HP];
-        T lap[4], pc[4];
         if (!first) {
 #pragma unroll
             for (int g = 0; g < (4 + 2 * HP) / 4; ++g) {
-                T t[4];
-                ld4(col - HP + 4 * g, t);
+                T tt[4];
+                ld4(col - HP + 4 * g, tt);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) zz[4 * g + q] = t[q];
+                for (int q = 0; q < 4; ++q) zz[4 * g + q] = tt[q];
             }
         } else {
 #pragma unroll
             for (int i = 0; i < 4 + 2 * HP; ++i) zz[i] = (T)0;
         }
+        T lap[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            pc[q] = zz[HP + q];
-            lap[q] = A::mul(c0, pc[q]);
-        }
+        for (int q = 0; q < 4; ++q) lap[q] = A::mul(c0, zz[HP + q]);
 #pragma unroll
         for (int k = 1; k <= H; ++k) {
-            T xm[4], xp[4];
+            T xm[4] = {0, 0, 0, 0}, xp[4] = {0, 0, 0, 0};
             if (!first) {
-                ld4(col - (size_t)k * S::SZ, xm);
-                ld4(col + (size_t)k * S::SZ, xp);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) { xm[q] = (T)0; xp[q] = (T)0; }
+                ld4(col - k * SZ, xm);
+                ld4(col + k * SZ, xp);
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const T ax = A::add(xp[q], xm[q]);
                 const T az = A::add(zz[HP + q + k], zz[HP + q - k]);
-                lap[q] = A::add(lap[q], A::add(A::mul(cx[k], ax), A::mul(cz[k], az)));
+                lap[q] = A::add(lap[q], A::add(A::mul((T)cx[k], ax), A::mul((T)cz[k], az)));
             }
         }
-
-        // Leapfrog with the sponge folded in.
-        const bool col_ok = (x >= H) && (x < nxe - H);
-        T val[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const T w = (T)__fmul_rn(wxv, wzv[q]);
+            const T w = (T)__fmul_rn(wxv, wz[q]);
             const T prev = A::mul(pp[q], w);
-            const T s = A::add(A::sub(A::mul((T)2, pc[q]), prev), A::mul((T)vd[q], lap[q]));
-            val[q] = (col_ok && row_ok[q]) ? A::mul(s, w) : (T)0;
+            const T s = A::add(A::sub(A::mul((T)2, zz[HP + q]), prev), A::mul(vd[q], lap[q]));
+            val[q] = A::mul(s, w);
+        }
+    }
+};
+
+
+// ------------------------------------------------------------- the tile
+// Computes one tile after its boxes have landed in the stage.
+template <typename T, int H, bool EXACT, int NWARP, int COLS>
+__device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ st, const TileInfo& t,
+                                             T* __restrict__ pcur, T* __restrict__ pnext, int ldz) {
+    using A = Arith<T, EXACT>;
+    using S = TileShape<T, H, NWARP, COLS>;
+    constexpr int HP = S::HP;
+    const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
+    const T* __restrict__ sm_pc = reinterpret_cast<const T*>(st + S::PC_OFF);
+    const T* __restrict__ sm_pp = reinterpret_cast<const T*>(st + S::PP_OFF);
+    const T* __restrict__ sm_vd = reinterpret_cast<const T*>(st + S::VD_OFF);
+    const float* __restrict__ sm_wx = reinterpret_cast<const float*>(st + S::WX_OFF);
+    const float* __restrict__ sm_wz = reinterpret_cast<const float*>(st + S::WZ_OFF);
+    const int* __restrict__ sm_cs = reinterpret_cast<const int*>(st + S::CS_OFF);
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int zr = t.z0 + 4 * lane;              // first of this thread's 4 rows
+    const int nxe = d.nxe, nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
+    const int it = t.it;
+    const bool fwd = t.fwd, first = t.first;
+    const bool lane_in = zr < nze;
+    const bool do_snap = t.do_snap, do_image = t.do_image;
+    const int snap_type = d.snap_type;
+
+    const T c0 = (T)d.c0;
+    const float* cx = d.cx;     // read from shared memory where used
+    const float* cz = d.cz;
+
+    bool row_ok[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) row_ok[q] = (zr + q >= H) && (zr + q < nze - H);
+    float wz[4];
+    {
+        const float4 w4 = *reinterpret_cast<const float4*>(sm_wz + 4 * lane);
+        wz[0] = w4.x; wz[1] = w4.y; wz[2] = w4.z; wz[3] = w4.w;
+    }
+    const bool lane_snap = lane_in && zr >= zs0 && zr < zs0 + lds;
+
+#pragma unroll
+    for (int c = 0; c < COLS; ++c) {
+        const int lx = warp * COLS + c;
+        const int x = t.x0 + lx;
+        if (x >= nxe) break;                     // warp-uniform
+        const T* col = sm_pc + (lx + H) * S::SZ + 4 * lane + HP;   // row zr of column x
+        const bool col_int = (x >= nb) && (x < nb + nx);
+        const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
+
+        // Backward stored steps: start the snapshot and image loads of this
+        // column first so their latency overlaps the stencil arithmetic.
+        T fs[4], Iv[4], Sv[4];
+        if (do_image && lane_snap && col_int) {
+            const size_t cell = (size_t)t.ksnap * nx * lds + ic;
+            const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
+            load_snapshot4<T>(d, cell, eidx, fs);
+            ld4(reinterpret_cast<const T*>(d.img) + ic, Iv);
+            ld4(reinterpret_cast<const T*>(d.ill) + ic, Sv);
         }
 
-        // Injection: the source (forward) or the receivers (backward) at cells
-        // whose taper is exactly 1, so adding after the damping matches the
-        // reference's inject-then-damp order bit for bit.
-        if (fwd) {
-            if (x == d.src_x) {
-                const T amp = (T)__ldg(d.wavelet + it);
+        T pp[4] = {0, 0, 0, 0}, vd[4];
+        ld4(sm_vd + lx * kTileZ + 4 * lane, vd);
+        if (!first) ld4(sm_pp + lx * kTileZ + 4 * lane, pp);
+        T val[4];
+        ColumnMath<T, H, EXACT, S::SZ, HP>::run(col, pp, vd, sm_wx[lx], wz, c0, cx, cz, first, val);
+        // the outer H-ring of the grid (and rows/columns past it) stays 0
+        const bool col_ok = (x >= H) && (x < nxe - H);
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (zr + q == d.src_z) val[q] = A::add(val[q], A::mul((T)vd[q], amp));
-            }
+        for (int q = 0; q < 4; ++q) val[q] = (col_ok && row_ok[q]) ? val[q] : (T)0;
+
+        // Injection at cells whose taper is exactly 1, so adding after the
+        // damping matches the reference's inject-then-damp order bit for bit.
+        if (fwd && x == d.src_x) {
+            const T amp = (T)__ldg(d.wavelet + it);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (zr + q == d.src_z) val[q] = A::add(val[q], A::mul(vd[q], amp));
         }
         // Receiver cells of this column: inject (backward) or record (forward
         // modelling).  Several receivers on one cell add in ascending ir order,
         // like the reference's sequential loop (backward.cpp:20-27).
-        const bool rec_fwd = fwd && (d.flags & kFlagRecord);
-        if (!fwd || rec_fwd) {
-            const int pb = __ldg(d.col_start + x), pe = __ldg(d.col_start + x + 1);
+        if (t.has_pts) {
+            const int pb = sm_cs[lx], pe = sm_cs[lx + 1];
             for (int j = pb; j < pe; ++j) {
                 const PointEntry e = d.pts[j];
 #pragma unroll
@@ -297,11 +361,11 @@ __device__ __forceinline__ void compute_tile(const ShotDesc& d, const T* __restr
                     if (e.z != zr + q) continue;
                     for (int r = 0; r < e.ir_count; ++r) {
                         const int ir = __ldg(d.pts_ir + e.ir_begin + r);
-                        if (rec_fwd) {
+                        if (fwd) {
                             d.rec_out[(size_t)ir * d.nt + it] = (float)val[q];
                         } else {
                             const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
-                            val[q] = A::add(val[q], A::mul((T)vd[q], tr));
+                            val[q] = A::add(val[q], A::mul(vd[q], tr));
                         }
                     }
                 }
@@ -309,19 +373,17 @@ __device__ __forceinline__ void compute_tile(const ShotDesc& d, const T* __restr
         }
 
         if (lane_in) {
-            st4(pn_col + zr, val);
+            st4(pnext + (uint32_t)x * (uint32_t)ldz + zr, val);
             if (first) {   // p^n of the first step is zero: clear the other level too
                 const T z4[4] = {0, 0, 0, 0};
-                st4(pcur + (size_t)x * ldz + zr, z4);
+                st4(pcur + (uint32_t)x * (uint32_t)ldz + zr, z4);
             }
         }
 
-        const bool col_int = (x >= d.nb) && (x < d.nb + d.nx);
         if (col_int && (do_snap || do_image)) {
-            const size_t cell = ((size_t)ksnap * d.nx + (x - d.nb)) * d.lds + (zr - d.zs0);
-            const size_t eidx = ((size_t)ksnap * d.nx + (x - d.nb)) * d.ntz + tz;
             if (do_snap) {
-                if (d.snap_type == kSnapF32 || d.snap_type == kSnapF64) {
+                const size_t cell = (size_t)t.ksnap * nx * lds + ic;
+                if (snap_type == kSnapF32 || snap_type == kSnapF64) {
                     if (lane_snap) st4cs(reinterpret_cast<T*>(d.snap) + cell, val);
                 } else {
                     // power-of-two scale per (snapshot, column, 128-row segment)
@@ -333,15 +395,18 @@ __device__ __forceinline__ void compute_tile(const ShotDesc& d, const T* __restr
                     for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
                     int e = 0;
                     if (amax > 0.f) {
-                        frexpf(amax, &e);          // amax <= 2^e
+                        // amax <= 2^e from the exponent field (subnormals: e = -126)
+                        const int ex = (__float_as_int(amax) >> 23) & 0xff;
+                        e = ex == 0 ? -126 : ex - 126;
                         e -= 15;                   // scaled max <= 2^15
                         e = e < -126 ? -126 : (e > 127 ? 127 : e);
                     }
+                    const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
                     if (lane == 0) d.snap_exp[eidx] = (int8_t)e;
                     if (lane_snap) {
                         const float inv = pow2f(-e);
                         uint2 packed;
-                        if (d.snap_type == kSnapF16) {
+                        if (snap_type == kSnapF16) {
                             const __half2 a = __floats2half2_rn((float)val[0] * inv, (float)val[1] * inv);
                             const __half2 b = __floats2half2_rn((float)val[2] * inv, (float)val[3] * inv);
                             packed.x = *reinterpret_cast<const uint32_t*>(&a);
@@ -357,50 +422,29 @@ __device__ __forceinline__ void compute_tile(const ShotDesc& d, const T* __restr
                 }
             }
             if (do_image && lane_snap) {
-                T f[4];
-                if (d.snap_type == kSnapF32 || d.snap_type == kSnapF64) {
-                    ld4cs(reinterpret_cast<const T*>(d.snap) + cell, f);
-                } else {
-                    const uint2 packed = __ldcs(reinterpret_cast<const uint2*>(
-                        reinterpret_cast<const uint16_t*>(d.snap) + cell));
-                    const float sc = pow2f((int)__ldg(d.snap_exp + eidx));
-                    float2 a, b;
-                    if (d.snap_type == kSnapF16) {
-                        a = __half22float2(*reinterpret_cast<const __half2*>(&packed.x));
-                        b = __half22float2(*reinterpret_cast<const __half2*>(&packed.y));
-                    } else {
-                        a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&packed.x));
-                        b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&packed.y));
-                    }
-                    f[0] = (T)(a.x * sc); f[1] = (T)(a.y * sc); f[2] = (T)(b.x * sc); f[3] = (T)(b.y * sc);
-                }
-                const size_t icell = (size_t)(x - d.nb) * d.lds + (zr - d.zs0);
-                T* img = reinterpret_cast<T*>(d.img) + icell;
-                T* ill = reinterpret_cast<T*>(d.ill) + icell;
-                T I[4], Sv[4];
-                ld4(img, I);
-                ld4(ill, Sv);
+                T* img = reinterpret_cast<T*>(d.img) + ic;
+                T* ill = reinterpret_cast<T*>(d.ill) + ic;
                 if (d.acc_mode == kAccPlain) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        I[q] = A::add(I[q], A::mul(f[q], val[q]));
-                        Sv[q] = A::add(Sv[q], A::mul(f[q], f[q]));
+                        Iv[q] = A::add(Iv[q], A::mul(fs[q], val[q]));
+                        Sv[q] = A::add(Sv[q], A::mul(fs[q], fs[q]));
                     }
                 } else {
                     // Kahan: sum + (term - comp), comp tracks the lost low part.
-                    T* imc = reinterpret_cast<T*>(d.img_c) + icell;
-                    T* ilc = reinterpret_cast<T*>(d.ill_c) + icell;
+                    T* imc = reinterpret_cast<T*>(d.img_c) + ic;
+                    T* ilc = reinterpret_cast<T*>(d.ill_c) + ic;
                     T Ic[4], Sc[4];
                     ld4(imc, Ic);
                     ld4(ilc, Sc);
                     using E = Arith<T, true>;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const T yi = E::sub(E::mul(f[q], val[q]), Ic[q]);
-                        const T ti = E::add(I[q], yi);
-                        Ic[q] = E::sub(E::sub(ti, I[q]), yi);
-                        I[q] = ti;
-                        const T ys = E::sub(E::mul(f[q], f[q]), Sc[q]);
+                        const T yi = E::sub(E::mul(fs[q], val[q]), Ic[q]);
+                        const T ti = E::add(Iv[q], yi);
+                        Ic[q] = E::sub(E::sub(ti, Iv[q]), yi);
+                        Iv[q] = ti;
+                        const T ys = E::sub(E::mul(fs[q], fs[q]), Sc[q]);
                         const T ts = E::add(Sv[q], ys);
                         Sc[q] = E::sub(E::sub(ts, Sv[q]), ys);
                         Sv[q] = ts;
@@ -408,58 +452,147 @@ __device__ __forceinline__ void compute_tile(const ShotDesc& d, const T* __restr
                     st4(imc, Ic);
                     st4(ilc, Sc);
                 }
-                st4(img, I);
+                st4(img, Iv);
                 st4(ill, Sv);
             }
         }
     }
 }
 
+// Fills one pipeline stage with tile `t`.  Executed by warp 0 only: lane 0
+// decodes what the tile does this step and publishes it as TileInfo, the lanes
+// copy the shot descriptor, the tile's taper weights and (for tiles with
+// receiver cells) the receiver-list offsets into shared memory, and lane 0
+// issues the TMA box loads against the stage's mbarrier.  An active tile
+// always loads (v dt)^2; p^n (with halo) and p^{n-1} are skipped on the first
+// step of a pass, where both are zero.
+template <typename T, int H, int NWARP, int COLS>
+__device__ __forceinline__ void load_stage(unsigned char* st, const CUtensorMap* map_pc, const CUtensorMap* map_box,
+                                           const StepParams& p, int t, long long g) {
+    using S = TileShape<T, H, NWARP, COLS>;
+    const int lane = threadIdx.x & 31;
+    const TileRef tr = p.tiles[t];
+    const ShotDesc& gd = p.descs[tr.slot];
+    {
+        const int* src = reinterpret_cast<const int*>(&gd);
+        int* dst = reinterpret_cast<int*>(st + S::DESC_OFF);
+        for (int i = lane; i < (int)(sizeof(ShotDesc) / 4); i += 32) dst[i] = src[i];
+    }
+    TileInfo ti{};
+    if (lane == 0) {
+        const long long n = g - gd.g0;
+        const int nt = gd.nt;
+        ti.active = n >= 0 && n < gd.total_steps;
+        ti.fwd = n < nt;
+        const int j = ti.fwd ? (int)n : (int)(n - nt);
+        ti.it = ti.fwd ? j : nt - 1 - j;
+        ti.first = j == 0;
+        ti.cur = j & 1;
+        ti.x0 = tr.tx * S::TX;
+        ti.z0 = tr.tz * kTileZ;
+        ti.tz = tr.tz;
+        const int si = gd.si;
+        const int ks = ti.it / si;
+        const bool stored = ks * si == ti.it;
+        const int flags = gd.flags;
+        ti.do_snap = ti.fwd && stored && (flags & kFlagSnapshots);
+        ti.do_image = !ti.fwd && stored && (flags & kFlagImage);
+        ti.ksnap = ks;
+        const bool pts_matter = !ti.fwd || (flags & kFlagRecord);
+        ti.has_pts = ti.active && pts_matter && gd.tile_pts[tr.tx * gd.ntz + tr.tz] != 0;
+        *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
+    }
+    ti.active = __shfl_sync(0xffffffffu, ti.active, 0);
+    if (!ti.active) return;
+    ti.first = __shfl_sync(0xffffffffu, ti.first, 0);
+    ti.cur = __shfl_sync(0xffffffffu, ti.cur, 0);
+    ti.has_pts = __shfl_sync(0xffffffffu, ti.has_pts, 0);
+    const int x0 = tr.tx * S::TX, z0 = tr.tz * kTileZ;
+    const int nxe = gd.nxe;
+    if (lane < S::TX) {
+        const int x = x0 + lane;
+        reinterpret_cast<float*>(st + S::WX_OFF)[lane] = x < nxe ? __ldg(gd.wx + x) : 0.f;
+    }
+    {
+        const int z = z0 + 4 * lane;
+        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (z < gd.nze) w = __ldg(reinterpret_cast<const float4*>(gd.wz + z));
+        reinterpret_cast<float4*>(st + S::WZ_OFF)[lane] = w;
+    }
+    if (ti.has_pts) {
+        for (int k = lane; k <= S::TX; k += 32) {
+            const int x = x0 + k < nxe ? x0 + k : nxe;
+            reinterpret_cast<int*>(st + S::CS_OFF)[k] = __ldg(gd.col_start + x);
+        }
+    }
+    if (lane == 0) {
+        uint64_t* bar = reinterpret_cast<uint64_t*>(st);
+        const int base = gd.field_slot * kFieldBuffers;
+        if (ti.first) {
+            mbar_arrive_expect_tx(bar, S::BOX_BYTES);
+        } else {
+            mbar_arrive_expect_tx(bar, S::PC_BYTES + 2 * S::BOX_BYTES);
+            tma_load_3d(st + S::PC_OFF, map_pc, bar, z0 - S::HP, x0 - H, base + ti.cur);
+            tma_load_3d(st + S::PP_OFF, map_box, bar, z0, x0, base + (ti.cur ^ 1));
+        }
+        tma_load_3d(st + S::VD_OFF, map_box, bar, z0, x0, base + 2);
+    }
+}
+
 // ------------------------------------------------------- per-step kernel
-// One launch = one time step of every tile in the tile list.
+// One launch = one time step of every tile in the tile list.  Persistent:
+// each CTA walks the list with stride gridDim.x through a two-stage pipeline,
+// so the loads of the next tile overlap the current tile's arithmetic.
 template <typename T, int H, bool EXACT, int NWARP, int COLS>
-__global__ void __launch_bounds__(NWARP * 32, 3)
-    step_kernel(const __grid_constant__ CUtensorMap tmap, const StepParams p) {
+__global__ void __launch_bounds__(NWARP * 32, sizeof(T) == 8 ? 1 : (COLS >= 4 ? 2 : 3))
+    step_kernel(const __grid_constant__ CUtensorMap map_pc, const __grid_constant__ CUtensorMap map_box,
+                const StepParams p) {
     using S = TileShape<T, H, NWARP, COLS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
-    ShotDesc* sd = reinterpret_cast<ShotDesc*>(smem_raw + 16);
-    T* tile = reinterpret_cast<T*>(smem_raw + S::DESC_BYTES);
 
-    if ((int)blockIdx.x >= p.ntiles) return;
-    const TileRef tr = p.tiles[blockIdx.x];
-    {   // stage the shot descriptor in shared memory (read by every thread)
-        const int* src = reinterpret_cast<const int*>(p.descs + tr.slot);
-        int* dst = reinterpret_cast<int*>(sd);
-        for (int i = threadIdx.x; i < (int)(sizeof(ShotDesc) / 4); i += blockDim.x) dst[i] = src[i];
-        if (threadIdx.x == 0) {
-            mbar_init(bar, 1);
-            fence_mbar_init();
-        }
-        __syncthreads();
+    int t = blockIdx.x;
+    if (t >= p.ntiles) return;
+    const long long g = *p.step_counter + p.step_offset;
+    const bool loader = threadIdx.x < 32;
+    if (threadIdx.x == 0) {
+        mbar_init(reinterpret_cast<uint64_t*>(smem_raw), 1);
+        mbar_init(reinterpret_cast<uint64_t*>(smem_raw + S::STAGE), 1);
+        fence_mbar_init();
     }
-    const ShotDesc& d = *sd;
-    const long long n = *p.step_counter + p.step_offset - d.g0;
-    if (n < 0 || n >= d.total_steps) return;   // shot idle this step
-    const bool fwd = n < d.nt;
-    const int j = fwd ? (int)n : (int)(n - d.nt);
-    const int it = fwd ? j : d.nt - 1 - j;
-    const bool first = (j == 0);
-    const int cur = j & 1;
+    __syncthreads();
+    if (loader) load_stage<T, H, NWARP, COLS>(smem_raw, &map_pc, &map_box, p, t, g);
+    __syncthreads();
+    uint32_t parity = 0;   // bit s: parity of the next wait on stage s
 
-    T* base = reinterpret_cast<T*>(p.fields) + (size_t)d.field_slot * p.slot_stride;
-    T* pcur = base + (size_t)cur * p.buf_stride;
-    T* pnext = base + (size_t)(cur ^ 1) * p.buf_stride;
-    const int x0 = tr.tx * S::TX, z0 = tr.tz * kTileZ;
-
-    if (!first) {
-        if (threadIdx.x == 0) {
-            mbar_arrive_expect_tx(bar, S::BYTES);
-            tma_load_3d(tile, &tmap, bar, z0 - S::HP, x0 - H, d.field_slot * 2 + cur);
+    for (int i = 0; t < p.ntiles; ++i) {
+        const int s = i & 1;
+        unsigned char* st = smem_raw + (s ? S::STAGE : 0);
+        unsigned char* st_next = smem_raw + (s ? 0 : S::STAGE);
+        const int tn = t + gridDim.x;
+        if (loader && tn < p.ntiles) load_stage<T, H, NWARP, COLS>(st_next, &map_pc, &map_box, p, tn, g);
+        const TileInfo info = *reinterpret_cast<const TileInfo*>(st + S::INFO_OFF);
+        if (info.active) {
+            bool timed_out =
+                !mbar_wait_bounded(reinterpret_cast<uint64_t*>(st), (parity >> s) & 1u, p.error_word, kWaitLimit);
+            parity ^= 1u << s;
+            // Collective decision: if any thread gave up, the whole CTA waits
+            // (bounded) for its in-flight copies and leaves together.
+            if (__syncthreads_or(timed_out)) {
+                mbar_wait_bounded(reinterpret_cast<uint64_t*>(st), ((parity >> s) & 1u) ^ 1u, p.error_word,
+                                  kWaitLimit);
+                if (tn < p.ntiles)
+                    mbar_wait_bounded(reinterpret_cast<uint64_t*>(st_next), (parity >> (s ^ 1)) & 1u,
+                                      p.error_word, 1 << 16);
+                return;
+            }
+            const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
+            T* base = reinterpret_cast<T*>(p.fields) + (size_t)d.field_slot * p.slot_stride;
+            compute_tile<T, H, EXACT, NWARP, COLS>(st, info, base + (size_t)info.cur * p.buf_stride,
+                                                   base + (size_t)(info.cur ^ 1) * p.buf_stride, p.ldz);
         }
-        if (!mbar_wait_bounded(bar, 0, p.error_word, kWaitLimit)) return;
+        __syncthreads();   // everyone is done with stage s, and stage s^1 is filled
+        t = tn;
     }
-    compute_tile<T, H, EXACT, NWARP, COLS>(d, tile, pcur, pnext, p.ldz, x0, z0, tr.tz, it, fwd, first);
 }
 
 // Advances the global step counter of a chunk (the last node of a captured

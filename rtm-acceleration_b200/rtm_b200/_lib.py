@@ -11,7 +11,7 @@ import os
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 ROOT_DIR = os.path.dirname(PKG_DIR)
-LIB_PATH = os.path.join(ROOT_DIR, "lib", "librtm_b200.so")
+LIB_PATH = os.environ.get("RTM_B200_LIBRARY") or os.path.join(ROOT_DIR, "lib", "librtm_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(ROOT_DIR), "include", "rtm_b200.h")
 
 OK, EINVAL, ENOMEM, ECUDA, ESTATE, ETIMEOUT, EUNSUPPORTED, EREJECTED, ENOTFOUND = 0, -1, -2, -3, -4, -5, -6, -7, -8

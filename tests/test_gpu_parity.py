@@ -222,8 +222,9 @@ def test_forward_backward_imaging_methods():
 def test_parameter_validation_errors():
     p, v, shots = small_problem(order=8, si=2, nt=50)
     from rtm_b200 import Engine
-    with pytest.raises(RTMError):
-        Engine("plain", RTMParams(order=7))
+    with Engine("plain", RTMParams(order=7)) as e:             # checked at setup, like the reference
+        with pytest.raises(RTMError):
+            e.setup(v, p.nx, p.nz, 10, 10, nt=50, dt=0.001)
     with Engine("plain", RTMParams(order=8, nb=4)) as e:     # nb < order/2+1
         with pytest.raises(RTMError):
             e.setup(v, p.nx, p.nz, 10, 10, nt=50, dt=0.001)
