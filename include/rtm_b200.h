@@ -115,6 +115,8 @@ typedef struct {
     double io, forward, backward, imaging, total, h2d, kernel, d2h;
     double cell_updates;      /* 2*nt*N_ext per migrated shot, summed          */
     double algorithmic_bytes; /* bytes the roofline counts, summed             */
+    double h2d_bytes;         /* host->device bytes the engine copied          */
+    double d2h_bytes;         /* device->host bytes the engine copied          */
     int    kernel_launches;   /* launches of this library's kernels            */
     int    shots;
 } rtm_b200_times;
@@ -162,7 +164,10 @@ RTM_B200_API int rtm_b200_setup(rtm_b200_engine* h, const float* vel, int nx, in
 
 /* Full migration (reference RTMEngine::migrate, include/rtm_engine.hpp:50-54,
  * src/rtm/rtm.cpp:83-103): image and illum (nx*nz, caller-owned) are
- * OVERWRITTEN with the zero-lag image and source illumination of all shots. */
+ * OVERWRITTEN with the zero-lag image and source illumination of all shots.
+ * Shot traces and the image/illum buffers may be host memory (pageable or
+ * page-locked) or device memory of the engine's GPU: device-resident inputs are
+ * read in place, page-locked ones are DMA'd without a staging copy. */
 RTM_B200_API int rtm_b200_migrate(rtm_b200_engine* h, const rtm_b200_shot* shots, int nshots, float* image,
                      float* illum);
 
@@ -235,6 +240,12 @@ RTM_B200_API float rtm_b200_points_per_wavelength(float vmin, float f0, float dx
  * shot->traces is ignored; `traces` (nrec*nt) is modified. */
 RTM_B200_API void rtm_b200_mute_direct_wave(const rtm_b200_shot* shot, float* traces, float v_surface,
                                             float t_pad, float t_taper);
+
+/* Copy-bandwidth probe on the engine's GPU (reference bandwidth probe,
+ * src/tools/bandwidth_probe_cuda.cu): copies bytes/2 to bytes/2, `iters` times,
+ * and reports read+write bytes per second.  A buffer well under the 126 MB L2
+ * measures L2 bandwidth, one of several GB measures HBM. */
+RTM_B200_API int rtm_b200_memory_probe(rtm_b200_engine* h, size_t bytes, int iters, double* gbps);
 
 /* ---- serving (no reference counterpart: the continuous-batching loop) ---- */
 

@@ -178,6 +178,10 @@ int rtm_b200_drain(rtm_b200_engine* h) {
 
 double rtm_b200_clock(const rtm_b200_engine* h) { return (h && h->e) ? h->e->clock() : 0.0; }
 
+int rtm_b200_memory_probe(rtm_b200_engine* h, size_t bytes, int iters, double* gbps) {
+    return guarded(h, [&](rtmb::Engine& e) { return e.memory_probe(bytes, iters, gbps); });
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------- host numerics

@@ -30,6 +30,28 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// True when p is device memory (the caller passed resident inputs/outputs).
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// True when p is page-locked host memory registered with CUDA (DMA-able as is).
+bool is_pinned_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
 
 Engine::Engine(const rtm_b200_config& cfg) : cfg_(cfg) {
@@ -323,7 +345,10 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     // Stage everything this job uploads in the slot's pinned buffer.
     std::vector<float> wx((size_t)gs.nxe);
     for (int i = 0; i < gs.nxe; ++i) wx[(size_t)i] = cerjan_taper(i, gs.nxe, gs.nb, m->alpha);
-    const size_t trace_elems = modelling ? 0 : (size_t)sh.nrec * sh.nt;
+    const bool dev_traces = !modelling && is_device_ptr(sh.traces);
+    const bool pinned_traces = !modelling && !dev_traces && is_pinned_ptr(sh.traces);
+    const size_t trace_h2d = (modelling || dev_traces) ? 0 : (size_t)sh.nrec * sh.nt;   // floats uploaded
+    const size_t trace_elems = pinned_traces ? 0 : trace_h2d;                           // floats staged
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off += round256(bytes); return o; };
     const size_t o_wx = take(wx.size() * 4);
@@ -369,7 +394,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     d.wx = sl.wx.get<float>();
     d.wz = m->wz.get<float>();
     d.wavelet = m->wavelet.get<float>();
-    d.traces = sl.traces.get<float>();
+    d.traces = dev_traces ? sh.traces : sl.traces.get<float>();
     d.col_start = sl.col_start.get<int>();
     d.tile_pts = sl.tile_pts.get<uint8_t>();
     d.pts = sl.pts.get<PointEntry>();
@@ -415,8 +440,12 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                                   cudaMemcpyHostToDevice, stream_));
     if (!geo.ir.empty())
         RTMB_CUDA(cudaMemcpyAsync(sl.ir.get(), st + o_ir, geo.ir.size() * 4, cudaMemcpyHostToDevice, stream_));
-    if (trace_elems)
-        RTMB_CUDA(cudaMemcpyAsync(sl.traces.get(), st + o_tr, trace_elems * 4, cudaMemcpyHostToDevice, stream_));
+    if (trace_h2d)
+        RTMB_CUDA(cudaMemcpyAsync(sl.traces.get(), pinned_traces ? (const void*)sh.traces : (const void*)(st + o_tr),
+                                  trace_h2d * 4, cudaMemcpyHostToDevice, stream_));
+    times.h2d_bytes += (double)trace_h2d * 4.0 +
+                       (double)(wx.size() * 4 + geo.col_start.size() * 4 + geo.pts.size() * sizeof(PointEntry) +
+                                geo.ir.size() * 4 + sizeof(ShotDesc) + tflags.size());
     RTMB_CUDA(cudaMemcpyAsync(sl.tile_pts.get(), st + o_tf, tflags.size(), cudaMemcpyHostToDevice, stream_));
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
@@ -707,9 +736,10 @@ int Engine::finalize_model_image(Model& m, float* img, float* ill, double* img64
             RTMB_CUDA(launch_extract_f32((const float*)si, g.lds, row0, d, g.nx, g.nz, 1, stream_));
             RTMB_CUDA(launch_extract_f32((const float*)ss, g.lds, row0, d + n, g.nx, g.nz, 1, stream_));
         }
+        if (img) RTMB_CUDA(cudaMemcpyAsync(img, d, n * 4, cudaMemcpyDefault, stream_));
+        if (ill) RTMB_CUDA(cudaMemcpyAsync(ill, d + n, n * 4, cudaMemcpyDefault, stream_));
+        times.d2h_bytes += (double)n * 4 * ((img && !is_device_ptr(img)) + (ill && !is_device_ptr(ill)));
         RTMB_CUDA(cudaStreamSynchronize(stream_));
-        if (img) RTMB_CUDA(cudaMemcpy(img, d, n * 4, cudaMemcpyDeviceToHost));
-        if (ill) RTMB_CUDA(cudaMemcpy(ill, d + n, n * 4, cudaMemcpyDeviceToHost));
     }
     if (img64 || ill64) {
         double* d = tmp.get<double>();
@@ -723,9 +753,10 @@ int Engine::finalize_model_image(Model& m, float* img, float* ill, double* img64
             RTMB_CUDA(launch_extract_f32((const float*)ss, g.lds, row0, f, g.nx, g.nz, 1, stream_));
             RTMB_CUDA(launch_widen(f, d + n, n, stream_));
         }
+        if (img64) RTMB_CUDA(cudaMemcpyAsync(img64, d, n * 8, cudaMemcpyDefault, stream_));
+        if (ill64) RTMB_CUDA(cudaMemcpyAsync(ill64, d + n, n * 8, cudaMemcpyDefault, stream_));
+        times.d2h_bytes += (double)n * 8 * ((img64 && !is_device_ptr(img64)) + (ill64 && !is_device_ptr(ill64)));
         RTMB_CUDA(cudaStreamSynchronize(stream_));
-        if (img64) RTMB_CUDA(cudaMemcpy(img64, d, n * 8, cudaMemcpyDeviceToHost));
-        if (ill64) RTMB_CUDA(cudaMemcpy(ill64, d + n, n * 8, cudaMemcpyDeviceToHost));
     }
     launches_ += 4;
     return RTM_B200_OK;
@@ -745,10 +776,11 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
     const GridDims& g = m.g;
     size_t freeb = 0, totalb = 0;
     RTMB_CUDA(cudaStreamSynchronize(stream_));
-    if (active_jobs() == 0) { arena_.release(); }
     RTMB_CUDA(cudaMemGetInfo(&freeb, &totalb));
+    // memory the engine already holds counts towards the budget it may use
+    const size_t held = pool_.bytes() + arena_.bytes();
     const size_t budget = cfg_.device_mem_budget > 0 ? (size_t)cfg_.device_mem_budget
-                                                     : (size_t)(0.9 * (double)(freeb + pool_.bytes()));
+                                                     : (size_t)(0.9 * (double)(freeb + held));
     size_t snap_max = 0, snap_sum = 0;
     for (auto& sh : m.shots) {
         const size_t b = snap_alloc_bytes(m, make_grid(sh.wnx, g.nz, g.nb, m.half));
@@ -769,11 +801,14 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
     size_t arena = cfg_.mode == RTM_B200_MODE_PLAIN ? snap_max
                                                     : (budget > (size_t)want * per_slot ? budget - (size_t)want * per_slot : 0);
     arena = std::max(arena, snap_max);
-    RTMB_CUDA(cudaMemGetInfo(&freeb, &totalb));
-    arena = std::min(arena, freeb > ((size_t)256 << 20) ? freeb - ((size_t)256 << 20) : 0);
-    if (arena < snap_max) return fail(RTM_B200_ENOMEM, "snapshot store for one shot does not fit device memory");
-    if (arena_.bytes() < arena || arena_.bytes() > arena + ((size_t)1 << 30)) {
+    // Keep the current store when it is big enough and not grossly oversized.
+    const bool keep_arena = arena_.bytes() >= arena && arena_.bytes() <= arena + arena / 4 + ((size_t)1 << 30);
+    if (!keep_arena) {
         arena_.release();
+        RTMB_CUDA(cudaMemGetInfo(&freeb, &totalb));
+        arena = std::min(arena, freeb > ((size_t)256 << 20) ? freeb - ((size_t)256 << 20) : 0);
+        if (arena < snap_max)
+            return fail(RTM_B200_ENOMEM, "snapshot store for one shot does not fit device memory");
         cudaError_t e = arena_.alloc(arena);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -922,6 +957,31 @@ int Engine::backward(const rtm_b200_shot* shot, const float* snaps, float* img, 
     }
     RTMB_TRY(check_device_error());
     RTMB_TRY(finalize_model_image(m, img, ill, nullptr, nullptr));
+    return RTM_B200_OK;
+}
+
+int Engine::memory_probe(size_t bytes, int iters, double* gbps) {
+    if (!gbps || bytes < 4096 || iters < 1) return fail(RTM_B200_EINVAL, "probe needs >= 4 KiB and >= 1 iteration");
+    RTMB_CUDA(cudaSetDevice(device_));
+    DevMem buf;
+    const size_t half = (bytes / 2) & ~(size_t)15;
+    if (buf.alloc(2 * half) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RTM_B200_ENOMEM, "probe buffer");
+    }
+    RTMB_CUDA(cudaMemsetAsync(buf.get(), 0, 2 * half, stream_));
+    const float4* src = buf.get<float4>();
+    float4* dst = reinterpret_cast<float4*>(buf.get<char>() + half);
+    const size_t n = half / 16;
+    for (int i = 0; i < 3; ++i) RTMB_CUDA(launch_copy_probe(src, dst, n, stream_));
+    RTMB_CUDA(cudaEventRecord(ev0_, stream_));
+    for (int i = 0; i < iters; ++i) RTMB_CUDA(launch_copy_probe(src, dst, n, stream_));
+    RTMB_CUDA(cudaEventRecord(ev1_, stream_));
+    RTMB_CUDA(cudaEventSynchronize(ev1_));
+    float ms = 0;
+    RTMB_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    *gbps = 2.0 * (double)half * iters / (ms * 1e-3) / 1e9;
+    launches_ += iters + 3;
     return RTM_B200_OK;
 }
 

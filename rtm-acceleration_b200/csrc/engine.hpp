@@ -104,6 +104,7 @@ public:
     int poll(long long ticket, rtm_b200_request_status* st, float* img, float* ill);
     int drain();
 
+    int memory_probe(size_t bytes, int iters, double* gbps);
     double clock() const;
     int num_snapshots() const { return model_ ? model_->nsnap : 0; }
     long long snapshot_bytes() const;

@@ -285,6 +285,15 @@ cudaError_t launch_slot_vdt2(void* dst, bool f64, int ldz, int nxe, const float*
     return cudaGetLastError();
 }
 
+__global__ void copy_probe_kernel(const float4* __restrict__ src, float4* __restrict__ dst, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+cudaError_t launch_copy_probe(const float4* src, float4* dst, size_t n, cudaStream_t s) {
+    copy_probe_kernel<<<148 * 8, 512, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
 __global__ void widen_kernel(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         dst[i] = (double)src[i];

@@ -68,6 +68,9 @@ cudaError_t launch_stack_f64(const double* I, const double* S, double* I64, doub
 cudaError_t launch_imaging_dense(const float* fwd, const float* bwd_ext, float* I, float* S, int nx, int nz,
                                  int nb, int nze, cudaStream_t s);
 
+// dst[i] = src[i] over n float4 elements (bandwidth probe).
+cudaError_t launch_copy_probe(const float4* src, float4* dst, size_t n, cudaStream_t s);
+
 // float -> double widening of a dense array.
 cudaError_t launch_widen(const float* src, double* dst, size_t n, cudaStream_t s);
 

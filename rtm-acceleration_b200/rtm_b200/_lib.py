@@ -42,8 +42,8 @@ class Shot(C.Structure):
 class Times(C.Structure):
     _fields_ = [("io", C.c_double), ("forward", C.c_double), ("backward", C.c_double), ("imaging", C.c_double),
                 ("total", C.c_double), ("h2d", C.c_double), ("kernel", C.c_double), ("d2h", C.c_double),
-                ("cell_updates", C.c_double), ("algorithmic_bytes", C.c_double), ("kernel_launches", C.c_int),
-                ("shots", C.c_int)]
+                ("cell_updates", C.c_double), ("algorithmic_bytes", C.c_double), ("h2d_bytes", C.c_double),
+                ("d2h_bytes", C.c_double), ("kernel_launches", C.c_int), ("shots", C.c_int)]
 
 
 class Request(C.Structure):
@@ -100,6 +100,7 @@ def load():
         "rtm_b200_poll": (C.c_int, [E, C.c_longlong, C.POINTER(RequestStatus), fp, fp]),
         "rtm_b200_drain": (C.c_int, [E]),
         "rtm_b200_clock": (C.c_double, [E]),
+        "rtm_b200_memory_probe": (C.c_int, [E, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

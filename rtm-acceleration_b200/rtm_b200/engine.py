@@ -51,6 +51,7 @@ class ShotRecord:
     traces: Optional[np.ndarray] = None
     window_x0: int = 0
     window_nx: int = 0
+    traces_ptr: int = 0        # raw address (device or page-locked host) used instead of `traces`
 
     @property
     def nrec(self) -> int:
@@ -71,12 +72,15 @@ def shots_to_c(shots: Sequence[ShotRecord], keep: list):
     for i, s in enumerate(shots):
         rx = np.ascontiguousarray(s.rx, np.float32).ravel()
         rz = np.ascontiguousarray(s.rz, np.float32).ravel()
-        tr = None if s.traces is None else np.ascontiguousarray(s.traces, np.float32).ravel()
+        tr = None if (s.traces is None or s.traces_ptr) else np.ascontiguousarray(s.traces, np.float32).ravel()
         keep.extend([rx, rz, tr])
         c = arr[i]
         c.sx, c.sz, c.nrec, c.nt, c.dt = float(s.sx), float(s.sz), rx.size, int(s.nt), float(s.dt)
         c.rx, c.rz = _fp(rx), _fp(rz)
-        c.traces = _fp(tr) if tr is not None else C.POINTER(C.c_float)()
+        if s.traces_ptr:
+            c.traces = C.cast(C.c_void_p(s.traces_ptr), C.POINTER(C.c_float))
+        else:
+            c.traces = _fp(tr) if tr is not None else C.POINTER(C.c_float)()
         c.window_x0, c.window_nx = int(s.window_x0), int(s.window_nx)
     return arr
 
@@ -161,6 +165,14 @@ class Engine:
         ill = np.zeros_like(img)
         self._check(self.lib.rtm_b200_migrate(self.h, arr, len(shots), _fp(img), _fp(ill)), "migrate")
         return img, ill
+
+    def migrate_into(self, shots: Sequence[ShotRecord], img_ptr: int, ill_ptr: int):
+        """migrate() writing nx*nz float32 results to raw addresses (device or host)."""
+        keep: list = []
+        arr = shots_to_c(shots, keep)
+        fp = C.POINTER(C.c_float)
+        self._check(self.lib.rtm_b200_migrate(self.h, arr, len(shots), C.cast(C.c_void_p(img_ptr), fp),
+                                              C.cast(C.c_void_p(ill_ptr), fp)), "migrate")
 
     def migrate_f64(self, shots: Sequence[ShotRecord]) -> Tuple[np.ndarray, np.ndarray]:
         keep: list = []
@@ -271,6 +283,12 @@ class Engine:
 
     def clock(self) -> float:
         return self.lib.rtm_b200_clock(self.h)
+
+    def memory_probe(self, nbytes: int, iters: int = 20) -> float:
+        """Copy bandwidth (read+write GB/s) over an nbytes buffer on the engine's GPU."""
+        g = C.c_double()
+        self._check(self.lib.rtm_b200_memory_probe(self.h, nbytes, iters, C.byref(g)), "memory_probe")
+        return g.value
 
 
 ENGINES = ("b200", "b200-batch", "b200-serve")
