@@ -247,6 +247,40 @@ RTM_B200_API void rtm_b200_mute_direct_wave(const rtm_b200_shot* shot, float* tr
  * measures L2 bandwidth, one of several GB measures HBM. */
 RTM_B200_API int rtm_b200_memory_probe(rtm_b200_engine* h, size_t bytes, int iters, double* gbps);
 
+/* ---- modelling without any GPU allocation ------------------------------- */
+
+/* One shot's model, parameters and device for rtm_b200_model_shot_static. */
+typedef struct {
+    const float* vel;           /* nx*nz zfast, host memory                      */
+    int          nx, nz;
+    float        dx, dz, ox, oz;
+    int          nb, order;
+    float        sponge_alpha, f0;
+    int          nt;
+    float        dt;
+    int          device;        /* CUDA device ordinal                          */
+} rtm_b200_static_problem;
+
+/* Forward modelling of one shot (the same kernel and results as
+ * rtm_b200_model_shots) that allocates no GPU memory at all.  This entry point
+ * has no counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: code running while a stream is captured into a CUDA graph,
+ * plugins whose host owns all device memory through its own pool, and loops
+ * that cannot afford the device-wide synchronisation of cudaMalloc/cudaFree.
+ * Its scratch (wavefields, tables, receiver lists) lives in a fixed 32 MiB
+ * array inside the library's device image, which every GPU that loads the
+ * library holds until the process exits; problems whose scratch exceeds it
+ * (roughly more than 2.6 million extended cells) are rejected with EINVAL and a
+ * message in `err`.  traces_out (nrec*nt, trace-major) may be host memory or
+ * device memory of `problem->device`.  The first call on a device looks up the
+ * array's device address, so make that first call before any stream capture.
+ * Calls share the array; calls that overlap on the GPU would race on it, and
+ * this function takes a per-device lock and returns only after its work is
+ * done, so calls from one process do not overlap.  Returns a status code; err
+ * (may be NULL) receives a message. */
+RTM_B200_API int rtm_b200_model_shot_static(const rtm_b200_static_problem* problem, const rtm_b200_shot* shot,
+                                            float* traces_out, char* err, size_t err_len);
+
 /* ---- serving (no reference counterpart: the continuous-batching loop) ---- */
 
 /* Queue a request; returns a ticket.  Rejected (EREJECTED) when it can never

@@ -53,6 +53,13 @@ class Request(C.Structure):
                 ("shots", C.POINTER(Shot)), ("arrival_time", C.c_double)]
 
 
+class StaticProblem(C.Structure):
+    _fields_ = [("vel", C.POINTER(C.c_float)), ("nx", C.c_int), ("nz", C.c_int), ("dx", C.c_float),
+                ("dz", C.c_float), ("ox", C.c_float), ("oz", C.c_float), ("nb", C.c_int), ("order", C.c_int),
+                ("sponge_alpha", C.c_float), ("f0", C.c_float), ("nt", C.c_int), ("dt", C.c_float),
+                ("device", C.c_int)]
+
+
 class RequestStatus(C.Structure):
     _fields_ = [("state", C.c_int), ("shots_done", C.c_int), ("submit_time", C.c_double),
                 ("start_time", C.c_double), ("finish_time", C.c_double), ("snapshot_bytes", C.c_double)]
@@ -101,6 +108,8 @@ def load():
         "rtm_b200_drain": (C.c_int, [E]),
         "rtm_b200_clock": (C.c_double, [E]),
         "rtm_b200_memory_probe": (C.c_int, [E, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
+        "rtm_b200_model_shot_static": (C.c_int, [C.POINTER(StaticProblem), C.POINTER(Shot), vp, C.c_char_p,
+                                                 C.c_size_t]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
