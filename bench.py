@@ -240,10 +240,13 @@ def run_b200_arm(args):
     from rtm_b200 import Engine, RTMParams, metrics
     from rtm_b200.engine import ShotRecord
 
-    # The survey has SHOTS_PER_GPU * world shots; rank r takes every world-th.
+    # The survey has SHOTS_PER_GPU * world shots; each rank takes a cost-balanced
+    # share (rtm_b200.shard: every rank computes the same assignment).
+    from rtm_b200 import shard
     w_all = make_workload(args.shots * world, args.nt)
+    all_shots = w_all.shots
     w = w_all
-    w.shots = w_all.shots[rank::world]
+    w.shots = shard.rank_shots(all_shots, rank, world, w.nx, w.nz, w.nb, w.nt)
     model_traces(w, local)
     nsh = len(w.shots)
     n_img = w.nx * w.nz
@@ -263,10 +266,10 @@ def run_b200_arm(args):
 
     def one_step(shots, img_ptr, ill_ptr):
         eng.migrate_into(shots, img_ptr, ill_ptr)
-        if dist is not None:
+        if dist is not None:   # the one exchange of the path: sum the ranks' stacks
             stack[:n_img].copy_(img)
             stack[n_img:].copy_(ill)
-            dist.all_reduce(stack)
+            shard.allreduce_stack(stack[:n_img], stack[n_img:])
 
     for _ in range(args.warmup):
         one_step(dev_shots, img.data_ptr(), ill.data_ptr())

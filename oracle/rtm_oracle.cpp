@@ -59,6 +59,7 @@ float ricker_f(float t, float f0) {
 template <typename T>
 struct Problem {
     int nx = 0, nz = 0, nb = 0, h = 0, nxe = 0, nze = 0, nt = 0, si = 1, nsnap = 0;
+    int nthreads = 1;     // host threads for the per-step loops (grids >= 64k cells)
     float dx = 0, dz = 0, ox = 0, oz = 0;
     T c0 = 0, cx[7] = {}, cz[7] = {};
     std::vector<T> vdt2, sponge, wavelet;
@@ -117,6 +118,7 @@ struct Problem {
         c0 = (T)(c[0] * (idx2 + idz2));
         for (int k = 1; k <= h; ++k) { cx[k] = (T)(c[k] * idx2); cz[k] = (T)(c[k] * idz2); }
         pp.assign(next(), 0); pc.assign(next(), 0); pn.assign(next(), 0);
+        nthreads = (next() >= 65536 && !omp_in_parallel()) ? omp_get_max_threads() : 1;
         return 0;
     }
 
@@ -130,8 +132,11 @@ struct Problem {
         return e(ix + nb, iz + nb);
     }
 
-    // Reference forward.cpp:29-50.  The outer h-ring is never written.
+    // Reference forward.cpp:29-50.  The outer h-ring is never written.  Every
+    // cell is independent, so columns are split over host threads (the result
+    // does not depend on the thread count).
     void step() {
+#pragma omp parallel for schedule(static) if (nthreads > 1) num_threads(nthreads)
         for (int ix = h; ix < nxe - h; ++ix) {
             for (int iz = h; iz < nze - h; ++iz) {
                 const size_t i = e(ix, iz);
@@ -148,8 +153,9 @@ struct Problem {
 
     // Reference forward.cpp:56-63: damp both p^n and p^{n+1} everywhere.
     void damp() {
-        const size_t n = next();
-        for (size_t i = 0; i < n; ++i) { pc[i] = pc[i] * sponge[i]; pn[i] = pn[i] * sponge[i]; }
+        const long n = (long)next();
+#pragma omp parallel for schedule(static) if (nthreads > 1) num_threads(nthreads)
+        for (long i = 0; i < n; ++i) { pc[i] = pc[i] * sponge[i]; pn[i] = pn[i] * sponge[i]; }
     }
 
     // rotate pp <- pc <- pn (reference forward.cpp:116-118).
