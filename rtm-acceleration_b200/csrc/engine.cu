@@ -241,9 +241,19 @@ int Engine::copy_shots(Model& m, const rtm_b200_shot* shots, int nshots, bool ne
 }
 
 // -------------------------------------------------------------- pool, slots
-int Engine::encode_map(int half, bool with_halo, CUtensorMap* out) {
+StepVariant Engine::variant(int half) const {
     StepVariant v;
-    v.f64 = f64_; v.half = half; v.cols = cols_;
+    v.f64 = f64_;
+    v.half = half;
+    v.cols = cols_;
+    v.exact = cfg_.arithmetic == RTM_B200_ARITH_IEEE;
+    auto it = nstage_.find(half);
+    v.nstage = it != nstage_.end() ? it->second : step_default_stages(v);
+    return v;
+}
+
+int Engine::encode_map(int half, bool with_halo, CUtensorMap* out) {
+    const StepVariant v = variant(half);
     const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)nslots_ * kFieldBuffers};
     const cuuint64_t strides[2] = {(cuuint64_t)ldz_cap_ * elem(), (cuuint64_t)ldz_cap_ * nxe_cap_ * elem()};
     const cuuint32_t box[3] = {(cuuint32_t)(with_halo ? step_box_z(v) : kTileZ),
@@ -291,6 +301,8 @@ int Engine::ensure_slot(int s, const Model& m, const ShotData& sh, const GridDim
     RTMB_CUDA(sl.col_start.reserve(sizeof(int) * (gs.nxe + 1)));
     RTMB_CUDA(sl.pts.reserve(sizeof(PointEntry) * nrec));
     RTMB_CUDA(sl.ir.reserve(sizeof(int) * nrec));
+    RTMB_CUDA(sl.rec_col.reserve(sizeof(int) * (gs.nxe + 1)));
+    RTMB_CUDA(sl.rec_z.reserve(sizeof(int) * nrec));
     if (!modelling) RTMB_CUDA(sl.traces.reserve(sizeof(float) * nrec * std::max(sh.nt, m.nt)));
     if (modelling) RTMB_CUDA(sl.rec.reserve(sizeof(float) * nrec * m.nt));
     if (cfg_.mode != RTM_B200_MODE_PLAIN && !modelling) {
@@ -341,6 +353,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
         for (int j = geo.col_start[(size_t)x]; j < geo.col_start[(size_t)x + 1]; ++j)
             tflags[(size_t)(x / TX) * gs.ntz + geo.pts[(size_t)j].z / kTileZ] = 1;
     RTMB_CUDA(sl.tile_pts.reserve(tflags.size()));
+    job.tile_pts = tflags;
 
     // Stage everything this job uploads in the slot's pinned buffer.
     std::vector<float> wx((size_t)gs.nxe);
@@ -355,6 +368,8 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     const size_t o_cs = take(geo.col_start.size() * 4);
     const size_t o_pts = take(geo.pts.size() * sizeof(PointEntry));
     const size_t o_ir = take(geo.ir.size() * 4);
+    const size_t o_rc = take(geo.rec_col.size() * 4);
+    const size_t o_rz = take(geo.rec_z.size() * 4);
     const size_t o_desc = take(sizeof(ShotDesc));
     const size_t o_tf = take(tflags.size());
     const size_t o_tr = take(trace_elems * 4);
@@ -368,6 +383,8 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     std::memcpy(st + o_cs, geo.col_start.data(), geo.col_start.size() * 4);
     if (!geo.pts.empty()) std::memcpy(st + o_pts, geo.pts.data(), geo.pts.size() * sizeof(PointEntry));
     if (!geo.ir.empty()) std::memcpy(st + o_ir, geo.ir.data(), geo.ir.size() * 4);
+    std::memcpy(st + o_rc, geo.rec_col.data(), geo.rec_col.size() * 4);
+    if (!geo.rec_z.empty()) std::memcpy(st + o_rz, geo.rec_z.data(), geo.rec_z.size() * 4);
     if (trace_elems) std::memcpy(st + o_tr, sh.traces, trace_elems * 4);
     std::memcpy(st + o_tf, tflags.data(), tflags.size());
 
@@ -399,6 +416,8 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     d.tile_pts = sl.tile_pts.get<uint8_t>();
     d.pts = sl.pts.get<PointEntry>();
     d.pts_ir = sl.ir.get<int>();
+    d.rec_col = sl.rec_col.get<int>();
+    d.rec_zs = sl.rec_z.get<int>();
     d.rec_out = sl.rec.get<float>();
     char* snap = arena_.get<char>() + snap_off;
     d.snap = snap_bytes ? snap : nullptr;
@@ -440,12 +459,16 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                                   cudaMemcpyHostToDevice, stream_));
     if (!geo.ir.empty())
         RTMB_CUDA(cudaMemcpyAsync(sl.ir.get(), st + o_ir, geo.ir.size() * 4, cudaMemcpyHostToDevice, stream_));
+    RTMB_CUDA(cudaMemcpyAsync(sl.rec_col.get(), st + o_rc, geo.rec_col.size() * 4, cudaMemcpyHostToDevice, stream_));
+    if (!geo.rec_z.empty())
+        RTMB_CUDA(cudaMemcpyAsync(sl.rec_z.get(), st + o_rz, geo.rec_z.size() * 4, cudaMemcpyHostToDevice, stream_));
     if (trace_h2d)
         RTMB_CUDA(cudaMemcpyAsync(sl.traces.get(), pinned_traces ? (const void*)sh.traces : (const void*)(st + o_tr),
                                   trace_h2d * 4, cudaMemcpyHostToDevice, stream_));
     times.h2d_bytes += (double)trace_h2d * 4.0 +
                        (double)(wx.size() * 4 + geo.col_start.size() * 4 + geo.pts.size() * sizeof(PointEntry) +
-                                geo.ir.size() * 4 + sizeof(ShotDesc) + tflags.size());
+                                geo.ir.size() * 4 + geo.rec_col.size() * 4 + geo.rec_z.size() * 4 +
+                                sizeof(ShotDesc) + tflags.size());
     RTMB_CUDA(cudaMemcpyAsync(sl.tile_pts.get(), st + o_tf, tflags.size(), cudaMemcpyHostToDevice, stream_));
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
@@ -521,12 +544,17 @@ int Engine::build_tiles() {
         if (!j.active) continue;
         const int ntx = (j.gs.nxe + TX - 1) / TX;
         auto& vec = by_half[j.m->half];
+        const ShotDesc& d = host_descs_[(size_t)s];
         for (int tz = 0; tz < j.gs.ntz; ++tz)
-            for (int tx = 0; tx < ntx; ++tx) vec.push_back(TileRef{s, tx, tz, 0});
+            for (int tx = 0; tx < ntx; ++tx)
+                vec.push_back(make_tile_ref(d, s, tx, tz, TX, j.tile_pts[(size_t)tx * j.gs.ntz + tz] != 0));
         sig.push_back(s);
         sig.push_back(j.m->half);
         sig.push_back(ntx);
         sig.push_back(j.gs.ntz);
+        sig.push_back(j.g0);
+        sig.push_back(j.total);
+        sig.push_back(d.flags);
     }
     tiles_dirty_ = false;
     if (sig == tile_sig_) return RTM_B200_OK;
@@ -549,10 +577,7 @@ int Engine::build_tiles() {
             RTMB_TRY(encode_map(g.half, false, &mp.box));
             maps_[g.half] = mp;
         }
-        StepVariant v;
-        v.f64 = f64_; v.half = g.half; v.cols = cols_;
-        v.exact = cfg_.arithmetic == RTM_B200_ARITH_IEEE;
-        RTMB_CUDA(prepare_step(v));
+        RTMB_CUDA(prepare_step(variant(g.half)));
     }
     return RTM_B200_OK;
 }
@@ -581,9 +606,7 @@ int Engine::run_chunk(int steps) {
     auto enqueue = [&]() -> int {
         for (int j = 0; j < steps; ++j)
             for (const Group& g : groups_) {
-                StepVariant v;
-                v.f64 = f64_; v.half = g.half; v.cols = cols_;
-                v.exact = cfg_.arithmetic == RTM_B200_ARITH_IEEE;
+                const StepVariant v = variant(g.half);
                 StepParams p{};
                 p.fields = pool_.get();
                 p.buf_stride = (long long)nxe_cap_ * ldz_cap_;
@@ -595,6 +618,7 @@ int Engine::run_chunk(int steps) {
                 p.step_counter = counter_.get<long long>();
                 p.step_offset = j;
                 p.error_word = errword_.get<int>();
+                p.pdl = 1;
                 const MapPair& mp = maps_[g.half];
                 RTMB_CUDA(launch_step(v, mp.pc, mp.box, p, stream_));
             }

@@ -35,6 +35,8 @@
 
 namespace rtmb {
 
+struct StepVariant;   // kernels.hpp
+
 struct ShotData {
     float sx = 0, sz = 0, dt = 0;
     int nrec = 0, nt = 0;
@@ -78,10 +80,11 @@ struct Job {
     float* rec_host = nullptr;
     size_t snap_off = 0, snap_bytes = 0;
     bool owns_snap = false;
+    std::vector<uint8_t> tile_pts;     // per (tx, tz): the tile holds receiver cells
 };
 
 struct Slot {
-    DevMem wx, col_start, pts, ir, traces, rec, acc, tile_pts;
+    DevMem wx, col_start, pts, ir, rec_col, rec_z, traces, rec, acc, tile_pts;
     PinnedMem stage;
     cudaEvent_t staged = nullptr;      // H2D from `stage` finished
 };
@@ -132,6 +135,7 @@ private:
     int ensure_pool(int nslots, int nxe_cap, int ldz_cap);
     int ensure_slot(int s, const Model& m, const ShotData& sh, const GridDims& gs, bool modelling);
     int encode_map(int half, bool with_halo, CUtensorMap* out);
+    StepVariant variant(int half) const;   // step-kernel variant for a stencil half-order
 
     // scheduling
     int start_job(int slot, Model* m, int shot, bool modelling, float* rec_host, int backward_only,
@@ -196,6 +200,7 @@ private:
     int graph_steps_ = 0;
     int launches_ = 0;
     int cols_ = 4;
+    std::map<int, int> nstage_;              // pipeline stages by half (autotuned), else default
     // backpressure: at most kChunksInFlight chunks queued ahead of the GPU
     static constexpr int kChunksInFlight = 3;
     cudaEvent_t chunk_ev_[kChunksInFlight] = {};

@@ -51,6 +51,18 @@ ShotGeometry build_geometry(float sx, float sz, int nrec, const float* rx, const
         i = j;
     }
     for (int x = 0; x < nxe; ++x) g.col_start[(size_t)x + 1] += g.col_start[(size_t)x];
+    // Per-receiver view of the same order (the kernel stages a tile's receivers
+    // from it): row of each receiver and receiver offsets per column.
+    g.rec_col.assign((size_t)nxe + 1, 0);
+    g.rec_z.reserve(g.ir.size());
+    for (int x = 0; x < nxe; ++x) {
+        int n = 0;
+        for (int j = g.col_start[(size_t)x]; j < g.col_start[(size_t)x + 1]; ++j) {
+            for (int r = 0; r < g.pts[(size_t)j].ir_count; ++r) g.rec_z.push_back(g.pts[(size_t)j].z);
+            n += g.pts[(size_t)j].ir_count;
+        }
+        g.rec_col[(size_t)x + 1] = g.rec_col[(size_t)x] + n;
+    }
     return g;
 }
 

@@ -12,6 +12,8 @@ struct ShotGeometry {
     std::vector<int> col_start;        // nxe+1 offsets into pts
     std::vector<PointEntry> pts;       // receiver cells sorted by (x, z)
     std::vector<int> ir;               // receivers of each cell, ascending
+    std::vector<int> rec_col;          // nxe+1 offsets into ir: receivers of the columns before x
+    std::vector<int> rec_z;            // extended row of each receiver, in ir order
     int nclamped = 0;                  // positions clamped onto the model edge
 };
 

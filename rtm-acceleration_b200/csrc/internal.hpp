@@ -80,6 +80,8 @@ struct ShotDesc {
     const uint8_t* tile_pts; // ntx*ntz flags: tile holds receiver cells
     const PointEntry* pts;
     const int* pts_ir;
+    const int* rec_col;      // nxe+1 receiver offsets per column (null: not staged)
+    const int* rec_zs;       // extended row of each receiver, pts_ir order
     float* rec_out;          // nrec * nt trace-major (modelling)
     void* snap;              // nsnap * nx * lds  (snap_type)
     int8_t* snap_exp;        // nsnap * nx * ntz  power-of-two scale exponents
@@ -91,12 +93,55 @@ struct ShotDesc {
 
 constexpr int kFieldBuffers = 3;     // p^n / p^{n+1}, p^{n-1}, (v dt)^2
 
-// One CTA's work item.
+// One receiver of a tile, staged in shared memory by the step kernel's producer.
+struct RecEntry {
+    int z;          // extended row of its cell
+    int ir;         // receiver index (trace row)
+    float tr;       // trace sample of this step (backward), unused when recording
+};
+
+// One CTA's work item: everything the step kernel's producer needs to decode
+// the tile's step and issue its TMA boxes, so that the issue waits on this one
+// 80-byte load only (the descriptor and tables follow in parallel).
 struct TileRef {
-    int slot;        // index into the descriptor array
-    int tx, tz;      // tile coordinates inside the shot's extended grid
+    int slot;            // index into the descriptor array
+    int tx, tz;          // tile coordinates inside the shot's extended grid
+    int has_pts;         // the tile holds receiver cells
+    int x0, z0;          // first column and row of the tile
+    int field_base;      // first field buffer of the shot's slot
+    int nt;              // time samples of the shot's time axis
+    long long g0;        // global step at which the job's forward step 0 runs
+    int total_steps;     // steps of the job
+    int si;              // store interval
+    const float* wx;     // the shot's x taper (nxe)
+    const float* wz;     // the model's z taper (ldz)
+    int flags;           // ShotFlags of the job
+    int nxe, nze;        // extended grid of the shot
     int pad;
 };
+static_assert(sizeof(TileRef) == 80, "TileRef layout");
+
+// Host-side construction of a TileRef from the slot's descriptor.
+inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int tile_x, bool has_pts) {
+    TileRef r{};
+    r.slot = slot;
+    r.tx = tx;
+    r.tz = tz;
+    r.has_pts = has_pts ? 1 : 0;
+    r.x0 = tx * tile_x;
+    r.z0 = tz * kTileZ;
+    r.field_base = d.field_slot * 3;
+    r.nt = d.nt;
+    r.g0 = d.g0;
+    r.total_steps = d.total_steps;
+    r.si = d.si;
+    r.wx = d.wx;
+    r.wz = d.wz;
+    r.flags = d.flags;
+    r.nxe = d.nxe;
+    r.nze = d.nze;
+    return r;
+}
 
 // Error bits written by the kernels into the engine's device error word.
 enum DeviceError : int {

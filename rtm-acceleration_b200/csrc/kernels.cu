@@ -14,35 +14,48 @@ __global__ void advance_counter_kernel(long long* counter, int by) {
 
 namespace {
 
+// Largest dynamic shared-memory request of a variant (kMaxStages stages, capped
+// at the 227 KB a CTA may use); set once, so any stage count up to it launches.
+template <typename T, int H, int COLS>
+int max_smem_impl() {
+    using S = TileShape<T, H, kStepWarps, COLS>;
+    int n = kMaxStages;
+    while (n > 2 && kCtrlBytes + n * S::STAGE > 227 * 1024) --n;
+    return kCtrlBytes + n * S::STAGE;
+}
+
 template <typename T, int H, bool EX, int COLS>
 cudaError_t attr_impl() {
-    using S = TileShape<T, H, kStepWarps, COLS>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
         attr_err = cudaFuncSetAttribute(step_kernel<T, H, EX, kStepWarps, COLS>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_impl<T, H, COLS>());
     });
     return attr_err;
 }
 
+// Resident CTAs per device for a stage count (the persistent grid size).
 template <typename T, int H, bool EX, int COLS>
-int max_grid_impl() {
+int max_grid_impl(int nstage) {
     using S = TileShape<T, H, kStepWarps, COLS>;
-    static std::once_flag once;
-    static int grid = 0;
-    std::call_once(once, [] {
+    static std::mutex mu;
+    static int cache[kMaxStages + 1] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (nstage < 2 || nstage > kMaxStages) return 0;
+    if (!cache[nstage]) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (attr_impl<T, H, EX, COLS>() == cudaSuccess &&
+        const int smem = kCtrlBytes + nstage * S::STAGE;
+        if (smem <= max_smem_impl<T, H, COLS>() && attr_impl<T, H, EX, COLS>() == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_kernel<T, H, EX, kStepWarps, COLS>,
-                                                          kStepThreads, S::SMEM) == cudaSuccess)
-            grid = sms * (per > 0 ? per : 1);
+                                                          kStepThreads, smem) == cudaSuccess && per > 0)
+            cache[nstage] = sms * per;
         else
-            grid = sms > 0 ? sms : 148;
-    });
-    return grid;
+            cache[nstage] = -1;
+    }
+    return cache[nstage] > 0 ? cache[nstage] : 0;
 }
 
 template <typename T, int H, bool EX, int COLS>
@@ -50,15 +63,19 @@ cudaError_t launch_impl(const CUtensorMap& mpc, const CUtensorMap& mpp, const St
     using S = TileShape<T, H, kStepWarps, COLS>;
     const cudaError_t e = attr_impl<T, H, EX, COLS>();
     if (e != cudaSuccess) return e;
-    const int cap = max_grid_impl<T, H, EX, COLS>();
-    const int grid = p.ntiles < cap ? p.ntiles : cap;
-    step_kernel<T, H, EX, kStepWarps, COLS><<<grid, kStepThreads, S::SMEM, s>>>(mpc, mpp, p);
-    return cudaGetLastError();
-}
-
-template <typename T, int H, bool EX, int COLS>
-int smem_impl() {
-    return TileShape<T, H, kStepWarps, COLS>::SMEM;
+    const int cap = max_grid_impl<T, H, EX, COLS>(p.nstage);
+    if (cap <= 0) return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(p.ntiles < cap ? p.ntiles : cap));
+    cfg.blockDim = dim3(kStepThreads);
+    cfg.dynamicSmemBytes = (size_t)(kCtrlBytes + p.nstage * S::STAGE);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p.pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, step_kernel<T, H, EX, kStepWarps, COLS>, mpc, mpp, p);
 }
 
 template <typename T, bool EX, int COLS>
@@ -75,14 +92,14 @@ cudaError_t by_half(int half, const CUtensorMap& a, const CUtensorMap& b, const 
 }
 
 template <typename T, bool EX, int COLS>
-int grid_by_half(int half) {
+int grid_by_half(int half, int nstage) {
     switch (half) {
-        case 1: return max_grid_impl<T, 1, EX, COLS>();
-        case 2: return max_grid_impl<T, 2, EX, COLS>();
-        case 3: return max_grid_impl<T, 3, EX, COLS>();
-        case 4: return max_grid_impl<T, 4, EX, COLS>();
-        case 5: return max_grid_impl<T, 5, EX, COLS>();
-        case 6: return max_grid_impl<T, 6, EX, COLS>();
+        case 1: return max_grid_impl<T, 1, EX, COLS>(nstage);
+        case 2: return max_grid_impl<T, 2, EX, COLS>(nstage);
+        case 3: return max_grid_impl<T, 3, EX, COLS>(nstage);
+        case 4: return max_grid_impl<T, 4, EX, COLS>(nstage);
+        case 5: return max_grid_impl<T, 5, EX, COLS>(nstage);
+        case 6: return max_grid_impl<T, 6, EX, COLS>(nstage);
         default: return 0;
     }
 }
@@ -113,26 +130,54 @@ cudaError_t prepare_step(const StepVariant& v) {
 bool step_variant_supported(const StepVariant& v) {
     if (v.half < 1 || v.half > kMaxHalf) return false;
     if (v.cols != 2 && v.cols != 4) return false;
-    return true;
+    if (v.nstage < 2 || v.nstage > kMaxStages) return false;
+    return step_smem_bytes(v) <= 227 * 1024;
 }
 
-int step_smem_bytes(const StepVariant& v) {
+int step_stage_bytes(const StepVariant& v) {
     const int elem = v.f64 ? 8 : 4;
     const int pc = step_box_z(v) * step_box_x(v) * elem;
     const int box = kTileZ * step_tile_x(v) * elem;
-    return 2 * (1408 + ((pc + 127) & ~127) + 2 * ((box + 127) & ~127));
+    return 1408 + ((pc + 127) & ~127) + 2 * ((box + 127) & ~127);
+}
+
+int step_smem_bytes(const StepVariant& v) { return kCtrlBytes + v.nstage * step_stage_bytes(v); }
+
+int step_default_stages(const StepVariant& v) {
+    // Deepest ring that still lets two FP32 CTAs share an SM (228 KB, 1 KB
+    // reserved per CTA); otherwise (FP64, or tiles too large for two CTAs) the
+    // deepest ring one CTA can hold.
+    StepVariant t = v;
+    const int per_sm = 228 * 1024;
+    if (!v.f64)
+        for (int n = kMaxStages; n >= 2; --n) {
+            t.nstage = n;
+            if (2 * (step_smem_bytes(t) + 1024) <= per_sm) return n;
+        }
+    for (int n = kMaxStages; n >= 2; --n) {
+        t.nstage = n;
+        if (step_smem_bytes(t) <= 227 * 1024) return n;
+    }
+    return 2;
 }
 
 int step_max_grid(const StepVariant& v) {
     if (!step_variant_supported(v)) return 0;
-    if (v.f64) return v.cols == 4 ? grid_by_half<double, false, 4>(v.half) : grid_by_half<double, false, 2>(v.half);
-    if (v.exact) return v.cols == 4 ? grid_by_half<float, true, 4>(v.half) : grid_by_half<float, true, 2>(v.half);
-    return v.cols == 4 ? grid_by_half<float, false, 4>(v.half) : grid_by_half<float, false, 2>(v.half);
+    if (v.f64)
+        return v.cols == 4 ? grid_by_half<double, false, 4>(v.half, v.nstage)
+                           : grid_by_half<double, false, 2>(v.half, v.nstage);
+    if (v.exact)
+        return v.cols == 4 ? grid_by_half<float, true, 4>(v.half, v.nstage)
+                           : grid_by_half<float, true, 2>(v.half, v.nstage);
+    return v.cols == 4 ? grid_by_half<float, false, 4>(v.half, v.nstage)
+                       : grid_by_half<float, false, 2>(v.half, v.nstage);
 }
 
-cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUtensorMap& mpp, const StepParams& p,
+cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUtensorMap& mpp, const StepParams& pin,
                         cudaStream_t s) {
-    if (!step_variant_supported(v) || p.ntiles <= 0) return cudaErrorInvalidValue;
+    if (!step_variant_supported(v) || pin.ntiles <= 0) return cudaErrorInvalidValue;
+    StepParams p = pin;
+    p.nstage = v.nstage;
     if (v.f64) {
         if (v.cols == 4) return by_half<double, false, 4>(v.half, mpc, mpp, p, s);
         return by_half<double, false, 2>(v.half, mpc, mpp, p, s);

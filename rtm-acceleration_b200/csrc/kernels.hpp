@@ -13,18 +13,22 @@ struct StepVariant {
     bool f64 = false;   // double fields (the FP64 run)
     int half = 4;       // order / 2
     bool exact = true;  // IEEE unfused float arithmetic (bit-identical path)
-    int cols = 4;       // columns per warp; tile is 128 rows x (8*cols) columns
+    int cols = 4;       // columns per consumer warp; tile is 128 rows x (8*cols) columns
+    int nstage = 3;     // shared-memory pipeline stages, 2..kMaxStages
 };
 
-constexpr int kStepWarps = 8;
-constexpr int kStepThreads = kStepWarps * 32;
+constexpr int kStepWarps = 8;                        // consumer warps
+constexpr int kStepThreads = (kStepWarps + 1) * 32;  // + the producer warp
 
 inline int step_tile_x(const StepVariant& v) { return kStepWarps * v.cols; }
 inline int step_halo_rows(const StepVariant& v) { return (v.half + 3) & ~3; }
 inline int step_box_z(const StepVariant& v) { return kTileZ + 2 * step_halo_rows(v); }
 inline int step_box_x(const StepVariant& v) { return step_tile_x(v) + 2 * v.half; }
+int step_stage_bytes(const StepVariant& v);
 int step_smem_bytes(const StepVariant& v);
 bool step_variant_supported(const StepVariant& v);
+// Deepest pipeline that keeps two CTAs per SM (FP32) / fits one CTA (FP64).
+int step_default_stages(const StepVariant& v);
 
 // Sets the kernel's shared-memory attribute (call before any stream capture).
 cudaError_t prepare_step(const StepVariant& v);
@@ -32,7 +36,9 @@ cudaError_t prepare_step(const StepVariant& v);
 // Resident CTAs of the persistent step kernel on this device (grid cap).
 int step_max_grid(const StepVariant& v);
 
-// Launch one time step over p.ntiles tiles (grid = min(ntiles, resident CTAs)).
+// Launch one time step over p.ntiles tiles (grid = min(ntiles, resident CTAs)),
+// as a programmatic dependent launch: its CTAs may start while the previous
+// kernel in the stream drains and wait in-kernel for it to finish.
 // map_pc: box of p^n with halo (step_box_z x step_box_x); map_box: box of
 // 128 x step_tile_x (p^{n-1} and (v dt)^2).  Both describe the field pool.
 cudaError_t launch_step(const StepVariant& v, const CUtensorMap& map_pc, const CUtensorMap& map_box,

@@ -132,6 +132,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     v.half = half;
     v.cols = 2;
     v.exact = true;
+    v.nstage = step_default_stages(v);
     const int TX = step_tile_x(v);
     const int ntx = (g.nxe + TX - 1) / TX;
     const ShotGeometry geo = build_geometry(shot->sx, shot->sz, shot->nrec, shot->rx, shot->rz, g.nx, g.nz, pr->dx,
@@ -140,9 +141,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     for (int x = 0; x < g.nxe; ++x)
         for (int j = geo.col_start[(size_t)x]; j < geo.col_start[(size_t)x + 1]; ++j)
             tflags[(size_t)(x / TX) * g.ntz + geo.pts[(size_t)j].z / kTileZ] = 1;
-    std::vector<TileRef> tiles;
-    for (int tz = 0; tz < g.ntz; ++tz)
-        for (int tx = 0; tx < ntx; ++tx) tiles.push_back(TileRef{0, tx, tz, 0});
+    const size_t ntiles = (size_t)ntx * g.ntz;
     const bool out_on_device = is_device_memory(traces_out);
     const size_t nrec = (size_t)std::max(shot->nrec, 0);
 
@@ -159,7 +158,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     const size_t o_ir = take(std::max<size_t>(geo.ir.size(), 1) * 4);
     const size_t o_tf = take(tflags.size());
     const size_t o_desc = take(sizeof(ShotDesc));
-    const size_t o_tiles = take(tiles.size() * sizeof(TileRef));
+    const size_t o_tiles = take(ntiles * sizeof(TileRef));
     const size_t o_ctr = take(sizeof(long long) + sizeof(int));
     const size_t o_rec = take(out_on_device ? 0 : nrec * pr->nt * 4);
     if (off > kStaticScratchBytes)
@@ -218,6 +217,11 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     if (!geo.ir.empty()) SS_CUDA(cudaMemcpy(base + o_ir, geo.ir.data(), geo.ir.size() * 4, cudaMemcpyHostToDevice));
     SS_CUDA(cudaMemcpy(base + o_tf, tflags.data(), tflags.size(), cudaMemcpyHostToDevice));
     SS_CUDA(cudaMemcpy(base + o_desc, &d, sizeof(ShotDesc), cudaMemcpyHostToDevice));
+    std::vector<TileRef> tiles;
+    tiles.reserve(ntiles);
+    for (int tz = 0; tz < g.ntz; ++tz)
+        for (int tx = 0; tx < ntx; ++tx)
+            tiles.push_back(make_tile_ref(d, 0, tx, tz, TX, tflags[(size_t)tx * g.ntz + tz] != 0));
     SS_CUDA(cudaMemcpy(base + o_tiles, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     SS_CUDA(cudaMemset(base + o_ctr, 0, sizeof(long long) + sizeof(int)));   // step counter and error word
 
@@ -243,7 +247,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     p.buf_stride = (long long)buf_elems;
     p.slot_stride = (long long)kFieldBuffers * buf_elems;
     p.ldz = g.ldz;
-    p.ntiles = (int)tiles.size();
+    p.ntiles = (int)ntiles;
     p.descs = reinterpret_cast<const ShotDesc*>(base + o_desc);
     p.tiles = reinterpret_cast<const TileRef*>(base + o_tiles);
     p.step_counter = reinterpret_cast<const long long*>(base + o_ctr);

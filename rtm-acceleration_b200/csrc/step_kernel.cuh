@@ -1,15 +1,18 @@
 // step_kernel.cuh -- the fused leapfrog time step for sm_100a.
 //
-// One CTA advances one 128-row x TX-column tile of one shot by one time step.
-// What the reference does in five passes per step (fd_time_step, inject_*,
-// apply_sponge, save_snapshot / imaging; reference src/rtm/forward.cpp:29-125,
+// A persistent, warp-specialised kernel advances every tile (128 rows x TX
+// columns of one shot) of the tile list by one time step.  What the reference
+// does in five passes per step (fd_time_step, inject_*, apply_sponge,
+// save_snapshot / imaging; reference src/rtm/forward.cpp:29-125,
 // backward.cpp:20-75, imaging.cpp:25-40) happens here in one:
 //
-//   1. one elected thread issues a 3D TMA tile load of p^n (tile + stencil halo)
-//      from HBM/L2 into shared memory, while every thread prefetches its own
-//      p^{n-1}, (v dt)^2 and taper values with 16-byte vector loads;
-//   2. each thread owns 4 consecutive depth cells (a float4) of COLS columns and
-//      evaluates the order-2H Laplacian from shared memory;
+//   1. a producer warp streams the CTA's tiles through a ring of shared-memory
+//      stages: per tile it stages the shot descriptor and taper weights and one
+//      lane issues 3D TMA box loads of p^n (tile + stencil halo), p^{n-1} and the
+//      shot's (v dt)^2 against the stage's "full" mbarrier;
+//   2. eight consumer warps wait on "full", each thread owns 4 consecutive depth
+//      cells (a float4) of COLS columns and evaluates the order-2H Laplacian
+//      from shared memory, then releases the stage on its "empty" mbarrier;
 //   3. p^{n+1} = w (2 p^n - w p^{n-1} + vdt2 lap) + injection, written in place
 //      over p^{n-1} (only the owning thread touches that cell, so two time
 //      levels suffice and there is no read/write race);
@@ -17,6 +20,10 @@
 //      BF16/FP16 with a power-of-two scale per 128-cell column segment) and the
 //      backward pass correlates with the stored snapshot (I += f b, S += f^2),
 //      either straight into the running image or into per-shot compensated sums.
+//
+// Successive step launches are programmatic dependent launches: a step's CTAs
+// wait in griddepcontrol.wait for the previous step to complete, so launch
+// processing overlaps the previous step's tail.
 //
 // Arithmetic: with EXACT=true every float operation is an IEEE round-to-nearest
 // add or multiply (no FMA contraction) in the same order as the reference's
@@ -47,6 +54,8 @@ struct StepParams {
     const long long* step_counter;  // global step of the first launch of a chunk
     int step_offset;                // this launch's offset within the chunk
     int* error_word;
+    int nstage;                     // pipeline stages (2..4) in dynamic shared memory
+    int pdl;                        // host side: launch as a programmatic dependent launch
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -160,20 +169,23 @@ struct Halo {
     static constexpr int HP = (H + 3) & ~3;
 };
 
-// Shared-memory stage of the pipelined step kernel:
-//   [0, 8)        mbarrier of this stage's TMA loads
-//   [16, 64)      TileInfo: what the tile does this step (written by warp 0)
+// One shared-memory stage of the pipelined step kernel:
+//   [0, 64)       TileInfo: what the tile does this step (written by the producer)
 //   [64, ...)     the tile's ShotDesc
 //   [WX_OFF, ..)  taper weights wx of the tile's TX columns
 //   [WZ_OFF, ..)  taper weights wz of the tile's 128 rows
-//   [CS_OFF, ..)  receiver-list offsets col_start[x0 .. x0+TX] (receiver tiles)
+//   [CS_OFF, ..)  receiver-cell offsets col_start[x0 .. x0+TX] (unstaged receivers)
+//   [RCS_OFF, ..) staged receivers: per-column offsets into the entries below
+//   [REC_OFF, ..) staged receivers: RecEntry {row, index, trace sample}
 //   [PC_OFF, ..)  TMA box of p^n with the stencil halo      (SZ x SX)
 //   [PP_OFF, ..)  TMA box of p^{n-1}                         (128 x TX)
 //   [VD_OFF, ..)  TMA box of the shot's (v dt)^2             (128 x TX)
 struct TileInfo {
     int active, fwd, first, it, cur, x0, z0, tz;
-    int do_snap, do_image, ksnap, has_pts;
+    int do_snap, do_image, ksnap, has_pts, rec_staged;
 };
+
+constexpr int kTileRec = 128;   // receivers a tile can stage in shared memory
 
 template <typename T, int H, int NWARP, int COLS>
 struct TileShape {
@@ -183,19 +195,22 @@ struct TileShape {
     static constexpr int SX = TX + 2 * H;        // columns of the p^n box
     static constexpr int PC_BYTES = SZ * SX * (int)sizeof(T);
     static constexpr int BOX_BYTES = kTileZ * TX * (int)sizeof(T);
-    static constexpr int INFO_OFF = 16;
+    static constexpr int INFO_OFF = 0;
     static constexpr int DESC_OFF = 64;
     static constexpr int WX_OFF = 512;
     static constexpr int WZ_OFF = WX_OFF + 128;
     static constexpr int CS_OFF = WZ_OFF + kTileZ * 4;
-    static constexpr int HDR = 1408;
+    static constexpr int RCS_OFF = 1408;
+    static constexpr int REC_OFF = RCS_OFF + 256;
+    static constexpr int HDR = REC_OFF + kTileRec * (int)sizeof(RecEntry);
     static constexpr int PC_OFF = HDR;
     static constexpr int PP_OFF = PC_OFF + ((PC_BYTES + 127) & ~127);
     static constexpr int VD_OFF = PP_OFF + ((BOX_BYTES + 127) & ~127);
     static constexpr int STAGE = VD_OFF + ((BOX_BYTES + 127) & ~127);
-    static constexpr int SMEM = 2 * STAGE;
     static_assert(TX <= 32, "wx staging holds at most 32 columns");
-    static_assert(CS_OFF + 4 * (TX + 1) <= HDR, "stage header overflow");
+    static_assert(CS_OFF + 4 * (TX + 1) <= RCS_OFF, "stage header overflow");
+    static_assert(4 * (TX + 1) <= REC_OFF - RCS_OFF, "staged receiver offsets overflow");
+    static_assert(HDR % 128 == 0, "TMA boxes must start 128-byte aligned");
     static_assert(INFO_OFF + sizeof(TileInfo) <= DESC_OFF, "tile info overflows its block");
     static_assert(DESC_OFF + sizeof(ShotDesc) <= WX_OFF, "descriptor overflows its block");
 };
@@ -353,19 +368,36 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
         // modelling).  Several receivers on one cell add in ascending ir order,
         // like the reference's sequential loop (backward.cpp:20-27).
         if (t.has_pts) {
-            const int pb = sm_cs[lx], pe = sm_cs[lx + 1];
-            for (int j = pb; j < pe; ++j) {
-                const PointEntry e = d.pts[j];
+            if (t.rec_staged) {
+                const int* __restrict__ rcs = reinterpret_cast<const int*>(st + S::RCS_OFF);
+                const RecEntry* __restrict__ re = reinterpret_cast<const RecEntry*>(st + S::REC_OFF);
+                const int kb = rcs[lx], ke = rcs[lx + 1];
+                for (int k = kb; k < ke; ++k) {
+                    const RecEntry e = re[k];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (e.z != zr + q) continue;
-                    for (int r = 0; r < e.ir_count; ++r) {
-                        const int ir = __ldg(d.pts_ir + e.ir_begin + r);
-                        if (fwd) {
-                            d.rec_out[(size_t)ir * d.nt + it] = (float)val[q];
-                        } else {
-                            const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
-                            val[q] = A::add(val[q], A::mul(vd[q], tr));
+                    for (int q = 0; q < 4; ++q) {
+                        if (e.z != zr + q) continue;
+                        if (fwd)
+                            d.rec_out[(size_t)e.ir * d.nt + it] = (float)val[q];
+                        else
+                            val[q] = A::add(val[q], A::mul(vd[q], (T)e.tr));
+                    }
+                }
+            } else {
+                const int pb = sm_cs[lx], pe = sm_cs[lx + 1];
+                for (int j = pb; j < pe; ++j) {
+                    const PointEntry e = d.pts[j];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (e.z != zr + q) continue;
+                        for (int r = 0; r < e.ir_count; ++r) {
+                            const int ir = __ldg(d.pts_ir + e.ir_begin + r);
+                            if (fwd) {
+                                d.rec_out[(size_t)ir * d.nt + it] = (float)val[q];
+                            } else {
+                                const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
+                                val[q] = A::add(val[q], A::mul(vd[q], tr));
+                            }
                         }
                     }
                 }
@@ -459,139 +491,251 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
     }
 }
 
-// Fills one pipeline stage with tile `t`.  Executed by warp 0 only: lane 0
-// decodes what the tile does this step and publishes it as TileInfo, the lanes
-// copy the shot descriptor, the tile's taper weights and (for tiles with
-// receiver cells) the receiver-list offsets into shared memory, and lane 0
-// issues the TMA box loads against the stage's mbarrier.  An active tile
-// always loads (v dt)^2; p^n (with halo) and p^{n-1} are skipped on the first
-// step of a pass, where both are zero.
+// ------------------------------------------------- pipeline control block
+// Shared memory of the step kernel: a 128-byte control block, then `nstage`
+// stages of TileShape::STAGE bytes each.
+//   [0, 32)    full[s]:  completes when the producer warp has written the
+//              stage header (all 32 lanes arrive) and the TMA boxes landed
+//   [32, 64)   empty[s]: completes when every consumer thread is done with it
+//   [64, 68)   abort flag (a bounded wait gave up somewhere in the CTA)
+//   [80, 96)   issued[s]: tiles the producer has issued into stage s
+constexpr int kMaxStages = 4;
+constexpr int kCtrlBytes = 128;
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Programmatic dependent launch: wait until the previous grid in the stream
+// has completed and its memory is visible, and let the next grid launch early
+// (its CTAs then only wait in griddep_wait for this grid to finish).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Bounded wait that also gives up as soon as another warp of the CTA aborted.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                                   int* err) {
+    long long n = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort_flag) return false;
+        if (++n > kWaitLimit) {
+            atomicOr(err, kErrTmaTimeout);
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Fills one stage with tile `t` (producer warp, all 32 lanes).  Lane 0 decodes
+// what the tile does this step and publishes it as TileInfo; the lanes copy
+// the shot descriptor, the tile's taper weights and (for tiles with receiver
+// cells) the receiver-list offsets into the stage; every lane then arrives on
+// the stage's full barrier (so each lane releases its own writes), lane 0 with
+// the byte count of the TMA boxes it issues.  An active tile always loads
+// (v dt)^2; p^n (with halo) and p^{n-1} are skipped on the first step of a
+// pass, where both are zero.  An inactive tile (its shot is not running at this
+// global step) only publishes TileInfo.
 template <typename T, int H, int NWARP, int COLS>
-__device__ __forceinline__ void load_stage(unsigned char* st, const CUtensorMap* map_pc, const CUtensorMap* map_box,
-                                           const StepParams& p, int t, long long g) {
+__device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, const CUtensorMap* map_pc,
+                                             const CUtensorMap* map_box, const StepParams& p, const TileRef& tr,
+                                             long long g) {
     using S = TileShape<T, H, NWARP, COLS>;
     const int lane = threadIdx.x & 31;
-    const TileRef tr = p.tiles[t];
+    // Decode the step (every lane, identically) and issue the boxes first: they
+    // depend on the TileRef only.
+    TileInfo ti{};
+    const long long n = g - tr.g0;
+    ti.active = n >= 0 && n < tr.total_steps;
+    if (!ti.active) {
+        if (lane == 0) *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
+        mbar_arrive(full);
+        return;
+    }
+    const int nt = tr.nt;
+    ti.fwd = n < nt;
+    const int j = ti.fwd ? (int)n : (int)(n - nt);
+    ti.it = ti.fwd ? j : nt - 1 - j;
+    ti.first = j == 0;
+    ti.cur = j & 1;
+    ti.x0 = tr.x0;
+    ti.z0 = tr.z0;
+    ti.tz = tr.tz;
+    const int ks = ti.it / tr.si;
+    const bool stored = ks * tr.si == ti.it;
+    ti.do_snap = ti.fwd && stored && (tr.flags & kFlagSnapshots);
+    ti.do_image = !ti.fwd && stored && (tr.flags & kFlagImage);
+    ti.ksnap = ks;
+    const bool pts_matter = !ti.fwd || (tr.flags & kFlagRecord);
+    ti.has_pts = pts_matter && tr.has_pts;
+    const int x0 = tr.x0, z0 = tr.z0;
+    if (lane == 0) {
+        *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
+        if (ti.first) {
+            mbar_expect_tx(full, S::BOX_BYTES);
+        } else {
+            mbar_expect_tx(full, S::PC_BYTES + 2 * S::BOX_BYTES);
+            tma_load_3d(st + S::PC_OFF, map_pc, full, z0 - S::HP, x0 - H, tr.field_base + ti.cur);
+            tma_load_3d(st + S::PP_OFF, map_box, full, z0, x0, tr.field_base + (ti.cur ^ 1));
+        }
+        tma_load_3d(st + S::VD_OFF, map_box, full, z0, x0, tr.field_base + 2);
+    }
+    // The descriptor and the per-tile tables, loaded in parallel by the lanes.
     const ShotDesc& gd = p.descs[tr.slot];
     {
         const int* src = reinterpret_cast<const int*>(&gd);
         int* dst = reinterpret_cast<int*>(st + S::DESC_OFF);
-        for (int i = lane; i < (int)(sizeof(ShotDesc) / 4); i += 32) dst[i] = src[i];
+        for (int i = lane; i < (int)(sizeof(ShotDesc) / 4); i += 32) dst[i] = __ldg(src + i);
     }
-    TileInfo ti{};
-    if (lane == 0) {
-        const long long n = g - gd.g0;
-        const int nt = gd.nt;
-        ti.active = n >= 0 && n < gd.total_steps;
-        ti.fwd = n < nt;
-        const int j = ti.fwd ? (int)n : (int)(n - nt);
-        ti.it = ti.fwd ? j : nt - 1 - j;
-        ti.first = j == 0;
-        ti.cur = j & 1;
-        ti.x0 = tr.tx * S::TX;
-        ti.z0 = tr.tz * kTileZ;
-        ti.tz = tr.tz;
-        const int si = gd.si;
-        const int ks = ti.it / si;
-        const bool stored = ks * si == ti.it;
-        const int flags = gd.flags;
-        ti.do_snap = ti.fwd && stored && (flags & kFlagSnapshots);
-        ti.do_image = !ti.fwd && stored && (flags & kFlagImage);
-        ti.ksnap = ks;
-        const bool pts_matter = !ti.fwd || (flags & kFlagRecord);
-        ti.has_pts = ti.active && pts_matter && gd.tile_pts[tr.tx * gd.ntz + tr.tz] != 0;
-        *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
-    }
-    ti.active = __shfl_sync(0xffffffffu, ti.active, 0);
-    if (!ti.active) return;
-    ti.first = __shfl_sync(0xffffffffu, ti.first, 0);
-    ti.cur = __shfl_sync(0xffffffffu, ti.cur, 0);
-    ti.has_pts = __shfl_sync(0xffffffffu, ti.has_pts, 0);
-    const int x0 = tr.tx * S::TX, z0 = tr.tz * kTileZ;
-    const int nxe = gd.nxe;
+    const int nxe = tr.nxe;
     if (lane < S::TX) {
         const int x = x0 + lane;
-        reinterpret_cast<float*>(st + S::WX_OFF)[lane] = x < nxe ? __ldg(gd.wx + x) : 0.f;
+        reinterpret_cast<float*>(st + S::WX_OFF)[lane] = x < nxe ? __ldg(tr.wx + x) : 0.f;
     }
     {
         const int z = z0 + 4 * lane;
         float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (z < gd.nze) w = __ldg(reinterpret_cast<const float4*>(gd.wz + z));
+        if (z < tr.nze) w = __ldg(reinterpret_cast<const float4*>(tr.wz + z));
         reinterpret_cast<float4*>(st + S::WZ_OFF)[lane] = w;
     }
     if (ti.has_pts) {
-        for (int k = lane; k <= S::TX; k += 32) {
-            const int x = x0 + k < nxe ? x0 + k : nxe;
-            reinterpret_cast<int*>(st + S::CS_OFF)[k] = __ldg(gd.col_start + x);
+        // Stage the tile's receivers (row, index and, backward, this step's
+        // trace sample) so consumers never chase the receiver lists in global
+        // memory; a tile with more than kTileRec receivers keeps the global path.
+        int staged = 0;
+        const int* rec_col = gd.rec_col;
+        if (rec_col) {
+            const int xe = x0 + S::TX < nxe ? x0 + S::TX : nxe;
+            const int r_lo = __ldg(rec_col + x0);
+            const int nrec = __ldg(rec_col + xe) - r_lo;
+            if (nrec <= kTileRec) {
+                staged = 1;
+                int* rcs = reinterpret_cast<int*>(st + S::RCS_OFF);
+                for (int k = lane; k <= S::TX; k += 32) {
+                    const int x = x0 + k < nxe ? x0 + k : nxe;
+                    rcs[k] = __ldg(rec_col + x) - r_lo;
+                }
+                const int* pts_ir = gd.pts_ir;
+                const int* rec_zs = gd.rec_zs;
+                const float* traces = gd.traces;
+                const int trace_nt = gd.trace_nt;
+                RecEntry* re = reinterpret_cast<RecEntry*>(st + S::REC_OFF);
+                for (int k = lane; k < nrec; k += 32) {
+                    RecEntry e;
+                    e.ir = __ldg(pts_ir + r_lo + k);
+                    e.z = __ldg(rec_zs + r_lo + k);
+                    e.tr = ti.fwd ? 0.f : __ldg(traces + (size_t)e.ir * trace_nt + ti.it);
+                    re[k] = e;
+                }
+            }
+        }
+        if (!staged)
+            for (int k = lane; k <= S::TX; k += 32) {
+                const int x = x0 + k < nxe ? x0 + k : nxe;
+                reinterpret_cast<int*>(st + S::CS_OFF)[k] = __ldg(gd.col_start + x);
+            }
+        if (lane == 0) reinterpret_cast<TileInfo*>(st + S::INFO_OFF)->rec_staged = staged;
+    }
+    // Stored backward steps: pull the tile's snapshot lines into L2 now, so the
+    // consumers' snapshot loads a few tiles later hit L2 instead of HBM.
+    if (ti.do_image) {
+        const char* snap = reinterpret_cast<const char*>(gd.snap);
+        const int snap_type = gd.snap_type, zs0 = gd.zs0, lds = gd.lds, nb = gd.nb, nx = gd.nx;
+        const int es = (snap_type == kSnapF32) ? 4 : (snap_type == kSnapF64 ? 8 : 2);
+        const int r0 = z0 > zs0 ? z0 : zs0;
+        const int r1 = z0 + kTileZ < zs0 + lds ? z0 + kTileZ : zs0 + lds;
+        if (snap && r1 > r0) {
+            const int bytes = (r1 - r0) * es;
+            const int lpc = (bytes + 127) >> 7;
+            for (int idx = lane; idx < S::TX * lpc; idx += 32) {
+                const int c = idx / lpc, l = idx - c * lpc;
+                const int xi = x0 + c - nb;
+                if (xi < 0 || xi >= nx) continue;
+                const char* a = snap + (((size_t)ti.ksnap * nx + xi) * lds + (r0 - zs0)) * es + (size_t)l * 128;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+            }
         }
     }
-    if (lane == 0) {
-        uint64_t* bar = reinterpret_cast<uint64_t*>(st);
-        const int base = gd.field_slot * kFieldBuffers;
-        if (ti.first) {
-            mbar_arrive_expect_tx(bar, S::BOX_BYTES);
-        } else {
-            mbar_arrive_expect_tx(bar, S::PC_BYTES + 2 * S::BOX_BYTES);
-            tma_load_3d(st + S::PC_OFF, map_pc, bar, z0 - S::HP, x0 - H, base + ti.cur);
-            tma_load_3d(st + S::PP_OFF, map_box, bar, z0, x0, base + (ti.cur ^ 1));
-        }
-        tma_load_3d(st + S::VD_OFF, map_box, bar, z0, x0, base + 2);
-    }
+    mbar_arrive(full);
 }
 
 // ------------------------------------------------------- per-step kernel
-// One launch = one time step of every tile in the tile list.  Persistent:
-// each CTA walks the list with stride gridDim.x through a two-stage pipeline,
-// so the loads of the next tile overlap the current tile's arithmetic.
+// One launch = one time step of every tile in the tile list.  Persistent and
+// warp-specialised: warp NWARP is the producer, which walks the CTA's tiles
+// (stride gridDim.x) and fills a ring of `nstage` shared-memory stages; warps
+// 0..NWARP-1 are consumers that compute each tile as soon as its stage is full
+// and release it.  No CTA-wide barrier inside the loop: the producer runs up to
+// nstage-1 tiles ahead of the consumers, so TMA latency hides behind compute.
 template <typename T, int H, bool EXACT, int NWARP, int COLS>
-__global__ void __launch_bounds__(NWARP * 32, sizeof(T) == 8 ? 1 : (COLS >= 4 ? 2 : 3))
+__global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
     step_kernel(const __grid_constant__ CUtensorMap map_pc, const __grid_constant__ CUtensorMap map_box,
                 const StepParams p) {
     using S = TileShape<T, H, NWARP, COLS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
+    uint64_t* empty = full + kMaxStages;
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(smem_raw + 64);
+    int* issued = reinterpret_cast<int*>(smem_raw + 80);
+    unsigned char* stages = smem_raw + kCtrlBytes;
+    const int nst = p.nstage;
 
-    int t = blockIdx.x;
-    if (t >= p.ntiles) return;
-    const long long g = *p.step_counter + p.step_offset;
-    const bool loader = threadIdx.x < 32;
+    if ((int)blockIdx.x >= p.ntiles) return;
     if (threadIdx.x == 0) {
-        mbar_init(reinterpret_cast<uint64_t*>(smem_raw), 1);
-        mbar_init(reinterpret_cast<uint64_t*>(smem_raw + S::STAGE), 1);
+        for (int s = 0; s < nst; ++s) {
+            mbar_init(full + s, 32);
+            mbar_init(empty + s, NWARP * 32);
+            issued[s] = 0;
+        }
+        *abort_flag = 0;
         fence_mbar_init();
     }
     __syncthreads();
-    if (loader) load_stage<T, H, NWARP, COLS>(smem_raw, &map_pc, &map_box, p, t, g);
-    __syncthreads();
-    uint32_t parity = 0;   // bit s: parity of the next wait on stage s
+    griddep_wait();
+    griddep_launch_dependents();
+    const long long g = *p.step_counter + p.step_offset;
+    const int warp = threadIdx.x >> 5;
 
-    for (int i = 0; t < p.ntiles; ++i) {
-        const int s = i & 1;
-        unsigned char* st = smem_raw + (s ? S::STAGE : 0);
-        unsigned char* st_next = smem_raw + (s ? 0 : S::STAGE);
-        const int tn = t + gridDim.x;
-        if (loader && tn < p.ntiles) load_stage<T, H, NWARP, COLS>(st_next, &map_pc, &map_box, p, tn, g);
-        const TileInfo info = *reinterpret_cast<const TileInfo*>(st + S::INFO_OFF);
-        if (info.active) {
-            bool timed_out =
-                !mbar_wait_bounded(reinterpret_cast<uint64_t*>(st), (parity >> s) & 1u, p.error_word, kWaitLimit);
-            parity ^= 1u << s;
-            // Collective decision: if any thread gave up, the whole CTA waits
-            // (bounded) for its in-flight copies and leaves together.
-            if (__syncthreads_or(timed_out)) {
-                mbar_wait_bounded(reinterpret_cast<uint64_t*>(st), ((parity >> s) & 1u) ^ 1u, p.error_word,
-                                  kWaitLimit);
-                if (tn < p.ntiles)
-                    mbar_wait_bounded(reinterpret_cast<uint64_t*>(st_next), (parity >> (s ^ 1)) & 1u,
-                                      p.error_word, 1 << 16);
-                return;
-            }
-            const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
-            T* base = reinterpret_cast<T*>(p.fields) + (size_t)d.field_slot * p.slot_stride;
-            compute_tile<T, H, EXACT, NWARP, COLS>(st, info, base + (size_t)info.cur * p.buf_stride,
-                                                   base + (size_t)(info.cur ^ 1) * p.buf_stride, p.ldz);
+    if (warp == NWARP) {
+        int i = 0;
+        TileRef cur = p.tiles[blockIdx.x];
+        TileRef nxt = cur;
+        for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++i) {
+            const int s = i % nst;
+            const int round = i / nst;
+            if (t + (int)gridDim.x < p.ntiles) nxt = p.tiles[t + gridDim.x];   // in flight while we wait
+            if (round > 0 && !mbar_wait_or_abort(empty + s, (round - 1) & 1, abort_flag, p.error_word)) break;
+            produce_tile<T, H, NWARP, COLS>(stages + (size_t)s * S::STAGE, full + s, &map_pc, &map_box, p, cur, g);
+            if ((threadIdx.x & 31) == 0) issued[s] = round + 1;
+            cur = nxt;
         }
-        __syncthreads();   // everyone is done with stage s, and stage s^1 is filled
-        t = tn;
+    } else {
+        int i = 0;
+        for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++i) {
+            const int s = i % nst;
+            const unsigned char* st = stages + (size_t)s * S::STAGE;
+            if (!mbar_wait_or_abort(full + s, (i / nst) & 1, abort_flag, p.error_word)) break;
+            const TileInfo info = *reinterpret_cast<const TileInfo*>(st + S::INFO_OFF);
+            if (info.active) {
+                const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
+                T* base = reinterpret_cast<T*>(p.fields) + (size_t)d.field_slot * p.slot_stride;
+                compute_tile<T, H, EXACT, NWARP, COLS>(st, info, base + (size_t)info.cur * p.buf_stride,
+                                                       base + (size_t)(info.cur ^ 1) * p.buf_stride, p.ldz);
+            }
+            mbar_arrive(empty + s);
+        }
+    }
+    __syncthreads();
+    // After an abort, copies the producer issued may still be in flight: wait
+    // (bounded) for the last phase of every stage before the CTA's shared
+    // memory goes away.
+    if (*abort_flag && threadIdx.x == 0) {
+        for (int s = 0; s < nst; ++s)
+            if (issued[s] > 0) mbar_wait_bounded(full + s, (uint32_t)((issued[s] - 1) & 1), p.error_word, 1 << 20);
     }
 }
 
