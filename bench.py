@@ -59,8 +59,8 @@ def parse_args():
     ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU, help="shots per GPU")
     ap.add_argument("--nt", type=int, default=0, help="override nt (0 = 4000)")
     ap.add_argument("--mode", default="batch", choices=["batch", "plain"])
-    ap.add_argument("--max-in-flight", type=int, default=4)
-    ap.add_argument("--tile-cols", type=int, default=32)
+    ap.add_argument("--max-in-flight", type=int, default=0, help="0 = the engine's default (16)")
+    ap.add_argument("--tile-cols", type=int, default=0, help="0 = autotuned")
     ap.add_argument("--snap", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--arith", default="ieee", choices=["ieee", "fma"])
     ap.add_argument("--no-fp64-check", action="store_true")

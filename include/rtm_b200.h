@@ -213,6 +213,12 @@ RTM_B200_API int rtm_b200_reset_times(rtm_b200_engine* h);
 /* Device identity (reference device_name(), include/rtm_engine.hpp:70-73). */
 RTM_B200_API int rtm_b200_device_name(const rtm_b200_engine* h, char* buf, size_t len);
 
+/* What the autotuner measured and chose, as JSON text: one record per job mix
+ * (stencil half-orders, tile rows, shots in flight), with the time per step of
+ * every candidate (columns per consumer warp, pipeline stages) and the pick.
+ * The reference has no autotuner; this reports the engine's own choices. */
+RTM_B200_API int rtm_b200_autotune_report(const rtm_b200_engine* h, char* buf, size_t len);
+
 /* Text of the last error on this handle (or of the last failed create when h
  * is NULL). */
 RTM_B200_API int rtm_b200_last_error(const rtm_b200_engine* h, char* buf, size_t len);

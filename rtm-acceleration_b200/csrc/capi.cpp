@@ -1,6 +1,7 @@
 // capi.cpp -- the extern "C" boundary of librtm_b200.so (declared in
 // include/rtm_b200.h).  Every entry point catches every C++ exception and turns
 // it into a status code; nothing throws across the ABI.
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -148,6 +149,27 @@ int rtm_b200_device_name(const rtm_b200_engine* h, char* buf, size_t len) {
     if (!h || !h->e) return RTM_B200_EINVAL;
     copy_str(h->e->device_name(), buf, len);
     return RTM_B200_OK;
+}
+
+int rtm_b200_autotune_report(const rtm_b200_engine* h, char* buf, size_t len) {
+    if (!h || !h->e || !buf) return RTM_B200_EINVAL;
+    std::string js = "[";
+    for (size_t i = 0; i < h->e->tune_log_.size(); ++i) {
+        const auto& r = h->e->tune_log_[i];
+        js += i ? ", {" : "{";
+        js += "\"key\": [";
+        for (size_t k = 0; k < r.key.size(); ++k) js += (k ? ", " : "") + std::to_string(r.key[k]);
+        js += "], \"us_per_step\": [";
+        for (size_t k = 0; k < r.us_per_step.size(); ++k) {
+            char t[32];
+            std::snprintf(t, sizeof t, "%s%.3f", k ? ", " : "", r.us_per_step[k]);
+            js += t;
+        }
+        js += "], \"cols\": " + std::to_string(r.cols) + ", \"stages\": " + std::to_string(r.stages) + "}";
+    }
+    js += "]";
+    copy_str(js, buf, len);
+    return js.size() < len ? RTM_B200_OK : RTM_B200_EINVAL;
 }
 
 int rtm_b200_last_error(const rtm_b200_engine* h, char* buf, size_t len) {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -68,6 +69,8 @@ Engine::~Engine() {
             if (s.staged) cudaEventDestroy(s.staged);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
+        if (tune_ev0_) cudaEventDestroy(tune_ev0_);
+        if (tune_ev1_) cudaEventDestroy(tune_ev1_);
         for (auto& e : chunk_ev_)
             if (e) cudaEventDestroy(e);
         for (auto& f : finishing_)
@@ -112,6 +115,12 @@ int Engine::init() {
     RTMB_CUDA(cudaMemsetAsync(errword_.get(), 0, sizeof(int), stream_));
     RTMB_CUDA(cudaStreamSynchronize(stream_));
     cols_ = cfg_.tile_cols == 32 ? 4 : 2;
+    autotune_ = cfg_.tile_cols == 0;
+    // Failure-detection test hook: the first step launch leaves this tile's
+    // stage empty, so the kernel's bounded wait must give up and report.
+    if (const char* st = std::getenv("RTM_B200_STALL_TILE")) stall_tile_ = std::atoi(st);
+    RTMB_CUDA(cudaEventCreate(&tune_ev0_));
+    RTMB_CUDA(cudaEventCreate(&tune_ev1_));
     inited_ = true;
     return RTM_B200_OK;
 }
@@ -247,8 +256,12 @@ StepVariant Engine::variant(int half) const {
     v.half = half;
     v.cols = cols_;
     v.exact = cfg_.arithmetic == RTM_B200_ARITH_IEEE;
-    auto it = nstage_.find(half);
-    v.nstage = it != nstage_.end() ? it->second : step_default_stages(v);
+    v.nstage = step_default_stages(v);
+    if (stage_override_ > 0) {
+        StepVariant t = v;
+        t.nstage = stage_override_;
+        if (step_variant_supported(t)) v.nstage = stage_override_;
+    }
     return v;
 }
 
@@ -345,15 +358,10 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                      geo.nclamped, sh.nrec + 1, (gs.nx - 1) * m->dx, (gs.nz - 1) * m->dz);
     RTMB_TRY(ensure_slot(s, *m, sh, gs, modelling));
     Slot& sl = slots_[(size_t)s];
-    // Which tiles hold receiver cells (the kernel only walks receiver lists there).
-    const int TX = kStepWarps * cols_;
-    const int ntx = (gs.nxe + TX - 1) / TX;
-    std::vector<uint8_t> tflags((size_t)ntx * gs.ntz, 0);
+    // Receiver cells (the tile list marks the tiles that hold any).
     for (int x = 0; x < gs.nxe; ++x)
         for (int j = geo.col_start[(size_t)x]; j < geo.col_start[(size_t)x + 1]; ++j)
-            tflags[(size_t)(x / TX) * gs.ntz + geo.pts[(size_t)j].z / kTileZ] = 1;
-    RTMB_CUDA(sl.tile_pts.reserve(tflags.size()));
-    job.tile_pts = tflags;
+            job.rec_cells.emplace_back(x, geo.pts[(size_t)j].z);
 
     // Stage everything this job uploads in the slot's pinned buffer.
     std::vector<float> wx((size_t)gs.nxe);
@@ -371,7 +379,6 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     const size_t o_rc = take(geo.rec_col.size() * 4);
     const size_t o_rz = take(geo.rec_z.size() * 4);
     const size_t o_desc = take(sizeof(ShotDesc));
-    const size_t o_tf = take(tflags.size());
     const size_t o_tr = take(trace_elems * 4);
     RTMB_CUDA(cudaEventSynchronize(sl.staged));   // previous upload from this buffer is done
     if (cudaSuccess != sl.stage.reserve(off)) {
@@ -386,13 +393,12 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     std::memcpy(st + o_rc, geo.rec_col.data(), geo.rec_col.size() * 4);
     if (!geo.rec_z.empty()) std::memcpy(st + o_rz, geo.rec_z.data(), geo.rec_z.size() * 4);
     if (trace_elems) std::memcpy(st + o_tr, sh.traces, trace_elems * 4);
-    std::memcpy(st + o_tf, tflags.data(), tflags.size());
 
     // Descriptor.
     ShotDesc d{};
     d.nxe = gs.nxe; d.nze = gs.nze; d.nx = gs.nx; d.nz = gs.nz; d.nb = gs.nb;
     d.model_x0 = sh.x0; d.win_nx = gs.nx;
-    d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz; d.ntx = ntx;
+    d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz; d.ntx = 0;   // tiles are listed per tile width (autotuned)
     d.nt = m->nt; d.si = m->si; d.nsnap = m->nsnap;
     job.first_phase_step = backward_only == 1 ? m->nt : 0;
     job.g0 = g_ - job.first_phase_step;
@@ -413,7 +419,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     d.wavelet = m->wavelet.get<float>();
     d.traces = dev_traces ? sh.traces : sl.traces.get<float>();
     d.col_start = sl.col_start.get<int>();
-    d.tile_pts = sl.tile_pts.get<uint8_t>();
+    d.tile_pts = nullptr;
     d.pts = sl.pts.get<PointEntry>();
     d.pts_ir = sl.ir.get<int>();
     d.rec_col = sl.rec_col.get<int>();
@@ -468,8 +474,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     times.h2d_bytes += (double)trace_h2d * 4.0 +
                        (double)(wx.size() * 4 + geo.col_start.size() * 4 + geo.pts.size() * sizeof(PointEntry) +
                                 geo.ir.size() * 4 + geo.rec_col.size() * 4 + geo.rec_z.size() * 4 +
-                                sizeof(ShotDesc) + tflags.size());
-    RTMB_CUDA(cudaMemcpyAsync(sl.tile_pts.get(), st + o_tf, tflags.size(), cudaMemcpyHostToDevice, stream_));
+                                sizeof(ShotDesc));
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
     // The slot's (v dt)^2 on the shot's extended grid (third field buffer).
@@ -543,11 +548,13 @@ int Engine::build_tiles() {
         const Job& j = jobs_[(size_t)s];
         if (!j.active) continue;
         const int ntx = (j.gs.nxe + TX - 1) / TX;
+        std::vector<uint8_t> tflags((size_t)ntx * j.gs.ntz, 0);
+        for (const auto& c : j.rec_cells) tflags[(size_t)(c.first / TX) * j.gs.ntz + c.second / kTileZ] = 1;
         auto& vec = by_half[j.m->half];
         const ShotDesc& d = host_descs_[(size_t)s];
         for (int tz = 0; tz < j.gs.ntz; ++tz)
             for (int tx = 0; tx < ntx; ++tx)
-                vec.push_back(make_tile_ref(d, s, tx, tz, TX, j.tile_pts[(size_t)tx * j.gs.ntz + tz] != 0));
+                vec.push_back(make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0));
         sig.push_back(s);
         sig.push_back(j.m->half);
         sig.push_back(ntx);
@@ -556,6 +563,8 @@ int Engine::build_tiles() {
         sig.push_back(j.total);
         sig.push_back(d.flags);
     }
+    sig.push_back(cols_);
+    sig.push_back(stage_override_);
     tiles_dirty_ = false;
     if (sig == tile_sig_) return RTM_B200_OK;
     tile_sig_ = sig;
@@ -571,15 +580,37 @@ int Engine::build_tiles() {
     RTMB_CUDA(tiles_.reserve(all.size() * sizeof(TileRef)));
     RTMB_CUDA(cudaMemcpy(tiles_.get(), all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     for (auto& g : groups_) {
-        if (!maps_.count(g.half)) {
+        const int mk = g.half * 16 + cols_;
+        if (!maps_.count(mk)) {
             MapPair mp;
             RTMB_TRY(encode_map(g.half, true, &mp.pc));
             RTMB_TRY(encode_map(g.half, false, &mp.box));
-            maps_[g.half] = mp;
+            maps_[mk] = mp;
         }
         RTMB_CUDA(prepare_step(variant(g.half)));
     }
     return RTM_B200_OK;
+}
+
+// The job mix a tuning result applies to: stencil half-orders present, tile
+// rows of the tallest shot, and the number of shots in flight (bucketed).
+std::vector<long long> Engine::tune_key() const {
+    std::vector<long long> k;
+    int n = 0, ntz = 0;
+    std::map<int, int> halves;
+    for (const auto& j : jobs_)
+        if (j.active) {
+            ++n;
+            ntz = std::max(ntz, j.gs.ntz);
+            halves[j.m->half] += 1;
+        }
+    for (auto& h : halves) k.push_back(h.first);
+    k.push_back(ntz);
+    int b = 1;
+    while (b < n) b *= 2;
+    k.push_back(b);
+    k.push_back(f64_ ? 1 : 0);
+    return k;
 }
 
 // After a failed run: drop every job, free its snapshot range and put the
@@ -600,7 +631,65 @@ void Engine::abort_jobs() {
     }
 }
 
+// Advances every job in flight by `steps` time steps.  With autotuning on
+// (tile_cols 0), the first chunk of a job mix not seen before is split: each
+// candidate (columns per warp, pipeline stages) runs a few real steps timed with
+// CUDA events, and the fastest is kept for the mix.  Every candidate computes
+// identical cells, so tuning costs no work.
 int Engine::run_chunk(int steps) {
+    if (!autotune_ || steps <= 0) return run_steps(steps);
+    if (tiles_dirty_ || groups_.empty()) {
+        const std::vector<long long> key = tune_key();
+        auto hit = tuned_.find(key);
+        if (hit != tuned_.end()) {
+            if (cols_ != hit->second.first || stage_override_ != hit->second.second) {
+                cols_ = hit->second.first;
+                stage_override_ = hit->second.second;
+                tiles_dirty_ = true;
+            }
+        } else {
+            const std::pair<int, int> cands[] = {{2, 0}, {2, 2}, {4, 0}, {4, 3}};
+            const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
+            const int k = std::min(16, steps / ncand);
+            if (k >= 4) {
+                TuneRecord rec;
+                rec.key = key;
+                double best = 1e300;
+                std::pair<int, int> pick = cands[0];
+                for (const auto& c : cands) {
+                    cols_ = c.first;
+                    stage_override_ = c.second;
+                    tiles_dirty_ = true;
+                    RTMB_CUDA(cudaStreamSynchronize(stream_));
+                    RTMB_TRY(build_tiles());
+                    bool ok = true;
+                    for (const auto& g : groups_) ok = ok && step_variant_supported(variant(g.half));
+                    if (!ok) { rec.us_per_step.push_back(-1.0); continue; }
+                    RTMB_CUDA(cudaEventRecord(tune_ev0_, stream_));
+                    RTMB_TRY(run_steps(k));
+                    RTMB_CUDA(cudaEventRecord(tune_ev1_, stream_));
+                    RTMB_CUDA(cudaEventSynchronize(tune_ev1_));
+                    float ms = 0.f;
+                    RTMB_CUDA(cudaEventElapsedTime(&ms, tune_ev0_, tune_ev1_));
+                    const double us = 1e3 * ms / k;
+                    rec.us_per_step.push_back(us);
+                    if (us < best) { best = us; pick = c; }
+                    steps -= k;
+                }
+                cols_ = pick.first;
+                stage_override_ = pick.second;
+                rec.cols = pick.first;
+                rec.stages = pick.second;
+                tuned_[key] = pick;
+                tune_log_.push_back(rec);
+                tiles_dirty_ = true;
+            }
+        }
+    }
+    return run_steps(steps);
+}
+
+int Engine::run_steps(int steps) {
     if (tiles_dirty_) RTMB_TRY(build_tiles());
     if (groups_.empty() || steps <= 0) return RTM_B200_OK;
     auto enqueue = [&]() -> int {
@@ -619,7 +708,12 @@ int Engine::run_chunk(int steps) {
                 p.step_offset = j;
                 p.error_word = errword_.get<int>();
                 p.pdl = 1;
-                const MapPair& mp = maps_[g.half];
+                p.stall_tile = -1;
+                if (stall_tile_ >= 0 && j == 0) {
+                    p.stall_tile = stall_tile_;
+                    stall_tile_ = -1;
+                }
+                const MapPair& mp = maps_[g.half * 16 + cols_];
                 RTMB_CUDA(launch_step(v, mp.pc, mp.box, p, stream_));
             }
         RTMB_CUDA(launch_advance_counter(counter_.get<long long>(), steps, stream_));
@@ -627,7 +721,7 @@ int Engine::run_chunk(int steps) {
     };
     cudaEvent_t& slot_ev = chunk_ev_[chunk_k_ % kChunksInFlight];
     if (chunk_k_ >= kChunksInFlight) RTMB_CUDA(cudaEventSynchronize(slot_ev));
-    const bool use_graph = cfg_.chunk_steps >= 0;
+    const bool use_graph = cfg_.chunk_steps >= 0 && stall_tile_ < 0;
     if (use_graph) {
         if (!graph_ || graph_sig_ != tile_sig_ || graph_steps_ != steps) {
             if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
@@ -815,7 +909,9 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
                             (size_t)4 * g.nxe * 3 + (size_t)m.nt * 4 * 2048;
     int want = 1;
     if (cfg_.mode != RTM_B200_MODE_PLAIN) {
-        want = cfg_.max_shots_in_flight > 0 ? cfg_.max_shots_in_flight : 256;
+        // 16 shots per launch measured best on the 1150 x 400 workload; more only
+        // when asked (the pool and the snapshot arena still bound it).
+        want = cfg_.max_shots_in_flight > 0 ? cfg_.max_shots_in_flight : 16;
         want = std::min(want, std::max(nshots, 1));
         const size_t snap_avg = nshots > 0 ? snap_sum / (size_t)nshots : snap_max;
         const size_t fit = budget / std::max<size_t>(per_slot + snap_avg, 1);

@@ -80,7 +80,7 @@ struct Job {
     float* rec_host = nullptr;
     size_t snap_off = 0, snap_bytes = 0;
     bool owns_snap = false;
-    std::vector<uint8_t> tile_pts;     // per (tx, tz): the tile holds receiver cells
+    std::vector<std::pair<int, int>> rec_cells;   // (x, z) extended cells holding receivers
 };
 
 struct Slot {
@@ -175,7 +175,7 @@ private:
     DevMem pool_;
     int nslots_ = 0, nxe_cap_ = 0, ldz_cap_ = 0;
     struct MapPair { CUtensorMap pc, box; };
-    std::map<int, MapPair> maps_;            // by half: p^n box with halo; 128 x TX box
+    std::map<int, MapPair> maps_;            // by (half, cols): p^n box with halo; 128 x TX box
     std::vector<Slot> slots_;
     std::vector<Job> jobs_;
     DevMem descs_;                           // ShotDesc[nslots]
@@ -200,7 +200,19 @@ private:
     int graph_steps_ = 0;
     int launches_ = 0;
     int cols_ = 4;
-    std::map<int, int> nstage_;              // pipeline stages by half (autotuned), else default
+    int stage_override_ = 0;
+    int stall_tile_ = -1;                    // failure-detection test hook (RTM_B200_STALL_TILE)                 // pipeline stages chosen by the autotuner (0 = default)
+    // Autotuner: the fastest (columns per warp, pipeline stages) measured on
+    // real steps, cached per job mix (stencil orders, tile rows, shots in flight).
+    bool autotune_ = false;
+    std::map<std::vector<long long>, std::pair<int, int>> tuned_;
+    std::vector<long long> tune_key() const;
+    int run_steps(int steps);
+    cudaEvent_t tune_ev0_ = nullptr, tune_ev1_ = nullptr;
+public:
+    struct TuneRecord { std::vector<long long> key; int cols, stages; std::vector<double> us_per_step; };
+    std::vector<TuneRecord> tune_log_;
+private:
     // backpressure: at most kChunksInFlight chunks queued ahead of the GPU
     static constexpr int kChunksInFlight = 3;
     cudaEvent_t chunk_ev_[kChunksInFlight] = {};

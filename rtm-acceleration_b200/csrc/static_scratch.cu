@@ -250,6 +250,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     p.ntiles = (int)ntiles;
     p.descs = reinterpret_cast<const ShotDesc*>(base + o_desc);
     p.tiles = reinterpret_cast<const TileRef*>(base + o_tiles);
+    p.stall_tile = -1;
     p.step_counter = reinterpret_cast<const long long*>(base + o_ctr);
     p.error_word = reinterpret_cast<int*>(base + o_ctr + sizeof(long long));
     for (int j = 0; j < pr->nt; ++j) {

@@ -56,6 +56,7 @@ struct StepParams {
     int* error_word;
     int nstage;                     // pipeline stages (2..4) in dynamic shared memory
     int pdl;                        // host side: launch as a programmatic dependent launch
+    int stall_tile;                 // failure-detection test: this tile is never produced (-1: none)
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -111,6 +112,42 @@ __device__ __forceinline__ void ld4cs(const double* p, double (&r)[4]) {
     r[0] = a.x; r[1] = a.y; r[2] = b.x; r[3] = b.y;
 }
 
+// Explicit global-space accesses for the consumers' field, snapshot and image
+// traffic: the stores are ordered only among themselves (no memory clobber), so
+// the compiler may issue the next column's shared-memory loads ahead of them.
+__device__ __forceinline__ size_t gaddr(const void* p) { return __cvta_generic_to_global(p); }
+__device__ __forceinline__ void stg4(float* p, const float (&r)[4]) {
+    asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(gaddr(p)), "f"(r[0]), "f"(r[1]), "f"(r[2]),
+                 "f"(r[3]));
+}
+__device__ __forceinline__ void stg4(double* p, const double (&r)[4]) {
+    asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(gaddr(p)), "d"(r[0]), "d"(r[1]));
+    asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(gaddr(p + 2)), "d"(r[2]), "d"(r[3]));
+}
+__device__ __forceinline__ void stg4cs(float* p, const float (&r)[4]) {
+    asm volatile("st.global.cs.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(gaddr(p)), "f"(r[0]), "f"(r[1]), "f"(r[2]),
+                 "f"(r[3]));
+}
+__device__ __forceinline__ void stg4cs(double* p, const double (&r)[4]) {
+    asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(gaddr(p)), "d"(r[0]), "d"(r[1]));
+    asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(gaddr(p + 2)), "d"(r[2]), "d"(r[3]));
+}
+__device__ __forceinline__ void stg_u2cs(void* p, uint2 v) {
+    asm volatile("st.global.cs.v2.u32 [%0], {%1, %2};" ::"l"(gaddr(p)), "r"(v.x), "r"(v.y));
+}
+__device__ __forceinline__ void stg1(float* p, float v) {
+    asm volatile("st.global.f32 [%0], %1;" ::"l"(gaddr(p)), "f"(v));
+}
+// Loads of data this launch does not write from another thread (image sums are
+// read and written by their owning thread only).
+__device__ __forceinline__ void ldg4(const float* p, float (&r)[4], int) {
+    asm("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]) : "l"(gaddr(p)));
+}
+__device__ __forceinline__ void ldg4(const double* p, double (&r)[4], int) {
+    asm("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(r[0]), "=d"(r[1]) : "l"(gaddr(p)));
+    asm("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(r[2]), "=d"(r[3]) : "l"(gaddr(p + 2)));
+}
+
 // 2^e as a float, exact for e in [-126, 127].
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
 
@@ -149,19 +186,29 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
-// Bounded wait: gives up after `limit` polls and reports it in the error word.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, long long limit) {
-    long long n = 0;
+// Wall-clock bound of every wait in the step kernel (globaltimer, ns).  A wait
+// that runs out sets an error bit and returns, so the kernel ends and the host
+// reports RTM_B200_ETIMEOUT instead of the GPU hanging.
+constexpr unsigned long long kWaitNs = 1000000000ull;   // 1 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: gives up after `ns` nanoseconds and reports it in the error word.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, unsigned long long ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity)) {
-        if (++n > limit) {
+        if (global_ns() - t0 > ns) {
             atomicOr(err, kErrTmaTimeout);
             return false;
         }
     }
     return true;
 }
-
-constexpr long long kWaitLimit = 1ll << 22;
 
 // Halo depth in rows, rounded up to 4 so the TMA box starts 16-byte aligned.
 template <int H>
@@ -286,12 +333,171 @@ struct ColumnMath {
 };
 
 
+// ------------------------------------------------------- column epilogue
+// Everything after the stencil arithmetic for one column of 4 rows per lane:
+// the zero outer ring, source and receiver injection (or trace recording), the
+// store of p^{n+1}, and on stored steps the snapshot store (forward) or the
+// imaging update (backward).  Shared by both step kernels.  Receivers: with
+// t.rec_staged, re[rkb..rke) are the column's staged receivers; otherwise
+// d.pts[rkb..rke) are its receiver cells in global memory.
+template <typename T, int H, bool EXACT>
+__device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInfo& t, int x, int zr, int lane,
+                                                bool lane_in, bool lane_snap, T (&val)[4], const T (&vd)[4],
+                                                const T (&fs)[4], T (&Iv)[4], T (&Sv)[4], int rkb, int rke,
+                                                const RecEntry* __restrict__ re, T* __restrict__ pcur,
+                                                T* __restrict__ pnext, int ldz) {
+    using A = Arith<T, EXACT>;
+    const int nxe = d.nxe, nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
+    const int it = t.it;
+    const bool fwd = t.fwd, first = t.first;
+    const bool do_snap = t.do_snap, do_image = t.do_image;
+    const int snap_type = d.snap_type;
+    const bool col_live = x < nxe;
+    const bool col_int = (x >= nb) && (x < nb + nx);
+    const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
+    // the outer H-ring of the grid (and rows/columns past it) stays 0
+    const bool col_ok = (x >= H) && (x < nxe - H);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool row_ok = (zr + q >= H) && (zr + q < nze - H);
+        val[q] = (col_ok && row_ok) ? val[q] : (T)0;
+    }
+
+    // Injection at cells whose taper is exactly 1, so adding after the
+    // damping matches the reference's inject-then-damp order bit for bit.
+    if (fwd && x == d.src_x) {
+        const T amp = (T)__ldg(d.wavelet + it);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (zr + q == d.src_z) val[q] = A::add(val[q], A::mul(vd[q], amp));
+    }
+    // Receiver cells of this column: inject (backward) or record (forward
+    // modelling).  Several receivers on one cell add in ascending ir order,
+    // like the reference's sequential loop (backward.cpp:20-27).
+    if (t.has_pts) {
+        if (t.rec_staged) {
+            for (int k = rkb; k < rke; ++k) {
+                const RecEntry e = re[k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (e.z != zr + q) continue;
+                    if (fwd)
+                        stg1(d.rec_out + (size_t)e.ir * d.nt + it, (float)val[q]);
+                    else
+                        val[q] = A::add(val[q], A::mul(vd[q], (T)e.tr));
+                }
+            }
+        } else {
+            for (int j = rkb; j < rke; ++j) {
+                const PointEntry e = d.pts[j];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (e.z != zr + q) continue;
+                    for (int r = 0; r < e.ir_count; ++r) {
+                        const int ir = __ldg(d.pts_ir + e.ir_begin + r);
+                        if (fwd) {
+                            stg1(d.rec_out + (size_t)ir * d.nt + it, (float)val[q]);
+                        } else {
+                            const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
+                            val[q] = A::add(val[q], A::mul(vd[q], tr));
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    if (lane_in && col_live) {
+        stg4(pnext + (uint32_t)x * (uint32_t)ldz + zr, val);
+        if (first) {   // p^n of the first step is zero: clear the other level too
+            const T z4[4] = {0, 0, 0, 0};
+            stg4(pcur + (uint32_t)x * (uint32_t)ldz + zr, z4);
+        }
+    }
+
+    if (col_int && (do_snap || do_image)) {
+        if (do_snap) {
+            const size_t cell = (size_t)t.ksnap * nx * lds + ic;
+            if (snap_type == kSnapF32 || snap_type == kSnapF64) {
+                if (lane_snap) stg4cs(reinterpret_cast<T*>(d.snap) + cell, val);
+            } else {
+                // power-of-two scale per (snapshot, column, 128-row segment)
+                float amax = 0.f;
+                if (lane_snap)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) amax = fmaxf(amax, fabsf((float)val[q]));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+                int e = 0;
+                if (amax > 0.f) {
+                    // amax <= 2^e from the exponent field (subnormals: e = -126)
+                    const int ex = (__float_as_int(amax) >> 23) & 0xff;
+                    e = ex == 0 ? -126 : ex - 126;
+                    e -= 15;                   // scaled max <= 2^15
+                    e = e < -126 ? -126 : (e > 127 ? 127 : e);
+                }
+                const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
+                if (lane == 0) d.snap_exp[eidx] = (int8_t)e;
+                if (lane_snap) {
+                    const float inv = pow2f(-e);
+                    uint2 packed;
+                    if (snap_type == kSnapF16) {
+                        const __half2 a = __floats2half2_rn((float)val[0] * inv, (float)val[1] * inv);
+                        const __half2 b = __floats2half2_rn((float)val[2] * inv, (float)val[3] * inv);
+                        packed.x = *reinterpret_cast<const uint32_t*>(&a);
+                        packed.y = *reinterpret_cast<const uint32_t*>(&b);
+                    } else {
+                        const __nv_bfloat162 a = __floats2bfloat162_rn((float)val[0] * inv, (float)val[1] * inv);
+                        const __nv_bfloat162 b = __floats2bfloat162_rn((float)val[2] * inv, (float)val[3] * inv);
+                        packed.x = *reinterpret_cast<const uint32_t*>(&a);
+                        packed.y = *reinterpret_cast<const uint32_t*>(&b);
+                    }
+                    stg_u2cs(reinterpret_cast<uint16_t*>(d.snap) + cell, packed);
+                }
+            }
+        }
+        if (do_image && lane_snap) {
+            T* img = reinterpret_cast<T*>(d.img) + ic;
+            T* ill = reinterpret_cast<T*>(d.ill) + ic;
+            if (d.acc_mode == kAccPlain) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    Iv[q] = A::add(Iv[q], A::mul(fs[q], val[q]));
+                    Sv[q] = A::add(Sv[q], A::mul(fs[q], fs[q]));
+                }
+            } else {
+                // Kahan: sum + (term - comp), comp tracks the lost low part.
+                T* imc = reinterpret_cast<T*>(d.img_c) + ic;
+                T* ilc = reinterpret_cast<T*>(d.ill_c) + ic;
+                T Ic[4], Sc[4];
+                ldg4(imc, Ic, 0);
+                ldg4(ilc, Sc, 0);
+                using E = Arith<T, true>;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const T yi = E::sub(E::mul(fs[q], val[q]), Ic[q]);
+                    const T ti = E::add(Iv[q], yi);
+                    Ic[q] = E::sub(E::sub(ti, Iv[q]), yi);
+                    Iv[q] = ti;
+                    const T ys = E::sub(E::mul(fs[q], fs[q]), Sc[q]);
+                    const T ts = E::add(Sv[q], ys);
+                    Sc[q] = E::sub(E::sub(ts, Sv[q]), ys);
+                    Sv[q] = ts;
+                }
+                stg4(imc, Ic);
+                stg4(ilc, Sc);
+            }
+            stg4(img, Iv);
+            stg4(ill, Sv);
+        }
+    }
+}
+
 // ------------------------------------------------------------- the tile
 // Computes one tile after its boxes have landed in the stage.
 template <typename T, int H, bool EXACT, int NWARP, int COLS>
 __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ st, const TileInfo& t,
                                              T* __restrict__ pcur, T* __restrict__ pnext, int ldz) {
-    using A = Arith<T, EXACT>;
     using S = TileShape<T, H, NWARP, COLS>;
     constexpr int HP = S::HP;
     const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
@@ -300,25 +506,19 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
     const T* __restrict__ sm_vd = reinterpret_cast<const T*>(st + S::VD_OFF);
     const float* __restrict__ sm_wx = reinterpret_cast<const float*>(st + S::WX_OFF);
     const float* __restrict__ sm_wz = reinterpret_cast<const float*>(st + S::WZ_OFF);
-    const int* __restrict__ sm_cs = reinterpret_cast<const int*>(st + S::CS_OFF);
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int zr = t.z0 + 4 * lane;              // first of this thread's 4 rows
-    const int nxe = d.nxe, nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
-    const int it = t.it;
-    const bool fwd = t.fwd, first = t.first;
+    const int nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
+    const bool first = t.first;
     const bool lane_in = zr < nze;
-    const bool do_snap = t.do_snap, do_image = t.do_image;
-    const int snap_type = d.snap_type;
+    const bool do_image = t.do_image;
 
     const T c0 = (T)d.c0;
     const float* cx = d.cx;     // read from shared memory where used
     const float* cz = d.cz;
 
-    bool row_ok[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) row_ok[q] = (zr + q >= H) && (zr + q < nze - H);
     float wz[4];
     {
         const float4 w4 = *reinterpret_cast<const float4*>(sm_wz + 4 * lane);
@@ -330,7 +530,6 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
     for (int c = 0; c < COLS; ++c) {
         const int lx = warp * COLS + c;
         const int x = t.x0 + lx;
-        if (x >= nxe) break;                     // warp-uniform
         const T* col = sm_pc + (lx + H) * S::SZ + 4 * lane + HP;   // row zr of column x
         const bool col_int = (x >= nb) && (x < nb + nx);
         const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
@@ -342,8 +541,8 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
             const size_t cell = (size_t)t.ksnap * nx * lds + ic;
             const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
             load_snapshot4<T>(d, cell, eidx, fs);
-            ld4(reinterpret_cast<const T*>(d.img) + ic, Iv);
-            ld4(reinterpret_cast<const T*>(d.ill) + ic, Sv);
+            ldg4(reinterpret_cast<const T*>(d.img) + ic, Iv, 0);
+            ldg4(reinterpret_cast<const T*>(d.ill) + ic, Sv, 0);
         }
 
         T pp[4] = {0, 0, 0, 0}, vd[4];
@@ -351,143 +550,14 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
         if (!first) ld4(sm_pp + lx * kTileZ + 4 * lane, pp);
         T val[4];
         ColumnMath<T, H, EXACT, S::SZ, HP>::run(col, pp, vd, sm_wx[lx], wz, c0, cx, cz, first, val);
-        // the outer H-ring of the grid (and rows/columns past it) stays 0
-        const bool col_ok = (x >= H) && (x < nxe - H);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) val[q] = (col_ok && row_ok[q]) ? val[q] : (T)0;
-
-        // Injection at cells whose taper is exactly 1, so adding after the
-        // damping matches the reference's inject-then-damp order bit for bit.
-        if (fwd && x == d.src_x) {
-            const T amp = (T)__ldg(d.wavelet + it);
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (zr + q == d.src_z) val[q] = A::add(val[q], A::mul(vd[q], amp));
-        }
-        // Receiver cells of this column: inject (backward) or record (forward
-        // modelling).  Several receivers on one cell add in ascending ir order,
-        // like the reference's sequential loop (backward.cpp:20-27).
+        int rkb = 0, rke = 0;
         if (t.has_pts) {
-            if (t.rec_staged) {
-                const int* __restrict__ rcs = reinterpret_cast<const int*>(st + S::RCS_OFF);
-                const RecEntry* __restrict__ re = reinterpret_cast<const RecEntry*>(st + S::REC_OFF);
-                const int kb = rcs[lx], ke = rcs[lx + 1];
-                for (int k = kb; k < ke; ++k) {
-                    const RecEntry e = re[k];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (e.z != zr + q) continue;
-                        if (fwd)
-                            d.rec_out[(size_t)e.ir * d.nt + it] = (float)val[q];
-                        else
-                            val[q] = A::add(val[q], A::mul(vd[q], (T)e.tr));
-                    }
-                }
-            } else {
-                const int pb = sm_cs[lx], pe = sm_cs[lx + 1];
-                for (int j = pb; j < pe; ++j) {
-                    const PointEntry e = d.pts[j];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (e.z != zr + q) continue;
-                        for (int r = 0; r < e.ir_count; ++r) {
-                            const int ir = __ldg(d.pts_ir + e.ir_begin + r);
-                            if (fwd) {
-                                d.rec_out[(size_t)ir * d.nt + it] = (float)val[q];
-                            } else {
-                                const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
-                                val[q] = A::add(val[q], A::mul(vd[q], tr));
-                            }
-                        }
-                    }
-                }
-            }
+            const int* __restrict__ off = reinterpret_cast<const int*>(st + (t.rec_staged ? S::RCS_OFF : S::CS_OFF));
+            rkb = off[lx];
+            rke = off[lx + 1];
         }
-
-        if (lane_in) {
-            st4(pnext + (uint32_t)x * (uint32_t)ldz + zr, val);
-            if (first) {   // p^n of the first step is zero: clear the other level too
-                const T z4[4] = {0, 0, 0, 0};
-                st4(pcur + (uint32_t)x * (uint32_t)ldz + zr, z4);
-            }
-        }
-
-        if (col_int && (do_snap || do_image)) {
-            if (do_snap) {
-                const size_t cell = (size_t)t.ksnap * nx * lds + ic;
-                if (snap_type == kSnapF32 || snap_type == kSnapF64) {
-                    if (lane_snap) st4cs(reinterpret_cast<T*>(d.snap) + cell, val);
-                } else {
-                    // power-of-two scale per (snapshot, column, 128-row segment)
-                    float amax = 0.f;
-                    if (lane_snap)
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) amax = fmaxf(amax, fabsf((float)val[q]));
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-                    int e = 0;
-                    if (amax > 0.f) {
-                        // amax <= 2^e from the exponent field (subnormals: e = -126)
-                        const int ex = (__float_as_int(amax) >> 23) & 0xff;
-                        e = ex == 0 ? -126 : ex - 126;
-                        e -= 15;                   // scaled max <= 2^15
-                        e = e < -126 ? -126 : (e > 127 ? 127 : e);
-                    }
-                    const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
-                    if (lane == 0) d.snap_exp[eidx] = (int8_t)e;
-                    if (lane_snap) {
-                        const float inv = pow2f(-e);
-                        uint2 packed;
-                        if (snap_type == kSnapF16) {
-                            const __half2 a = __floats2half2_rn((float)val[0] * inv, (float)val[1] * inv);
-                            const __half2 b = __floats2half2_rn((float)val[2] * inv, (float)val[3] * inv);
-                            packed.x = *reinterpret_cast<const uint32_t*>(&a);
-                            packed.y = *reinterpret_cast<const uint32_t*>(&b);
-                        } else {
-                            const __nv_bfloat162 a = __floats2bfloat162_rn((float)val[0] * inv, (float)val[1] * inv);
-                            const __nv_bfloat162 b = __floats2bfloat162_rn((float)val[2] * inv, (float)val[3] * inv);
-                            packed.x = *reinterpret_cast<const uint32_t*>(&a);
-                            packed.y = *reinterpret_cast<const uint32_t*>(&b);
-                        }
-                        __stcs(reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(d.snap) + cell), packed);
-                    }
-                }
-            }
-            if (do_image && lane_snap) {
-                T* img = reinterpret_cast<T*>(d.img) + ic;
-                T* ill = reinterpret_cast<T*>(d.ill) + ic;
-                if (d.acc_mode == kAccPlain) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        Iv[q] = A::add(Iv[q], A::mul(fs[q], val[q]));
-                        Sv[q] = A::add(Sv[q], A::mul(fs[q], fs[q]));
-                    }
-                } else {
-                    // Kahan: sum + (term - comp), comp tracks the lost low part.
-                    T* imc = reinterpret_cast<T*>(d.img_c) + ic;
-                    T* ilc = reinterpret_cast<T*>(d.ill_c) + ic;
-                    T Ic[4], Sc[4];
-                    ld4(imc, Ic);
-                    ld4(ilc, Sc);
-                    using E = Arith<T, true>;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const T yi = E::sub(E::mul(fs[q], val[q]), Ic[q]);
-                        const T ti = E::add(Iv[q], yi);
-                        Ic[q] = E::sub(E::sub(ti, Iv[q]), yi);
-                        Iv[q] = ti;
-                        const T ys = E::sub(E::mul(fs[q], fs[q]), Sc[q]);
-                        const T ts = E::add(Sv[q], ys);
-                        Sc[q] = E::sub(E::sub(ts, Sv[q]), ys);
-                        Sv[q] = ts;
-                    }
-                    st4(imc, Ic);
-                    st4(ilc, Sc);
-                }
-                st4(img, Iv);
-                st4(ill, Sv);
-            }
-        }
+        column_epilogue<T, H, EXACT>(d, t, x, zr, lane, lane_in, lane_snap, val, vd, fs, Iv, Sv, rkb, rke,
+                                     reinterpret_cast<const RecEntry*>(st + S::REC_OFF), pcur, pnext, ldz);
     }
 }
 
@@ -520,10 +590,11 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 // Bounded wait that also gives up as soon as another warp of the CTA aborted.
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                                    int* err) {
-    long long n = 0;
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort_flag) return false;
-        if (++n > kWaitLimit) {
+        if (global_ns() - t0 > kWaitNs) {
             atomicOr(err, kErrTmaTimeout);
             *abort_flag = 1;
             return false;
@@ -709,8 +780,13 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
             const int round = i / nst;
             if (t + (int)gridDim.x < p.ntiles) nxt = p.tiles[t + gridDim.x];   // in flight while we wait
             if (round > 0 && !mbar_wait_or_abort(empty + s, (round - 1) & 1, abort_flag, p.error_word)) break;
-            produce_tile<T, H, NWARP, COLS>(stages + (size_t)s * S::STAGE, full + s, &map_pc, &map_box, p, cur, g);
-            if ((threadIdx.x & 31) == 0) issued[s] = round + 1;
+            // Failure-detection test: a tile whose stage is never filled makes the
+            // consumers' bounded wait run out (no copy is in flight for it).
+            if (t != p.stall_tile) {
+                produce_tile<T, H, NWARP, COLS>(stages + (size_t)s * S::STAGE, full + s, &map_pc, &map_box, p, cur,
+                                                g);
+                if ((threadIdx.x & 31) == 0) issued[s] = round + 1;
+            }
             cur = nxt;
         }
     } else {
@@ -735,7 +811,8 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
     // memory goes away.
     if (*abort_flag && threadIdx.x == 0) {
         for (int s = 0; s < nst; ++s)
-            if (issued[s] > 0) mbar_wait_bounded(full + s, (uint32_t)((issued[s] - 1) & 1), p.error_word, 1 << 20);
+            if (issued[s] > 0)
+                mbar_wait_bounded(full + s, (uint32_t)((issued[s] - 1) & 1), p.error_word, kWaitNs / 4);
     }
 }
 

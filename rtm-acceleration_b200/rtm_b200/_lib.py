@@ -97,6 +97,7 @@ def load():
         "rtm_b200_reset_times": (C.c_int, [E]),
         "rtm_b200_device_name": (C.c_int, [E, C.c_char_p, C.c_size_t]),
         "rtm_b200_last_error": (C.c_int, [E, C.c_char_p, C.c_size_t]),
+        "rtm_b200_autotune_report": (C.c_int, [E, C.c_char_p, C.c_size_t]),
         "rtm_b200_stencil_coefficients": (C.c_int, [C.c_int, fp]),
         "rtm_b200_max_stable_dt": (C.c_float, [C.c_float, C.c_float, C.c_float, C.c_int]),
         "rtm_b200_ricker": (C.c_float, [C.c_float, C.c_float]),

@@ -241,6 +241,13 @@ class Engine:
         self.lib.rtm_b200_device_name(self.h, buf, 256)
         return buf.value.decode()
 
+    def autotune_report(self) -> list:
+        """Candidates the autotuner timed per job mix and what it chose."""
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        self._check(self.lib.rtm_b200_autotune_report(self.h, buf, 1 << 16), "autotune_report")
+        return json.loads(buf.value.decode())
+
     def times(self) -> dict:
         t = L.Times()
         self._check(self.lib.rtm_b200_get_times(self.h, C.byref(t)), "get_times")
