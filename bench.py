@@ -65,6 +65,10 @@ def parse_args():
     ap.add_argument("--arith", default="ieee", choices=["ieee", "fma"])
     ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
+                    help="config2 is the contract line; the others print one extra JSON line each")
+    ap.add_argument("--plain-shots", type=int, default=64, help="config3: shots timed on the plain engine")
+    ap.add_argument("--requests", type=int, default=24, help="config5: requests in the stream")
     return ap.parse_args()
 
 
@@ -384,8 +388,192 @@ def run_b200_arm(args):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------ other workloads
+def _timed_migrate(eng, shots, f64=False):
+    """One migration timed with the engine's CUDA events (device seconds)."""
+    eng.reset_times()
+    out = eng.migrate_f64(shots) if f64 else eng.migrate(shots)
+    return out, eng.times()
+
+
+def _model(w, device, shots=None):
+    from rtm_b200 import Engine, RTMParams
+    shots = shots if shots is not None else w.shots
+    p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=1)
+    with Engine("batch", p, device=device, max_shots_in_flight=16) as e:
+        e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+        tr = e.model_shots(shots)
+    for s, t in zip(shots, tr):
+        s.traces = t
+
+
+def run_config3(args):
+    """256 shots on uneven aperture windows (400-1150 columns of the
+    1150 x 400 model), orders 8 and 12: the batched engine (FP32 and BF16
+    snapshots, autotuned) against the plain one-shot-at-a-time engine."""
+    import torch
+    from rtm_b200 import Engine, RTMParams, metrics, synth
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    nshots = args.shots if args.shots != SHOTS_PER_GPU else 256
+    for order in (8, 12):
+        w = synth.config3(nshots=nshots, order=order)
+        _model(w, dev)
+        p = RTMParams(nb=w.nb, order=order, f0=w.f0, store_interval=w.store_interval)
+        res, times, images = {}, {}, {}
+        for name, mode, snap in (("batch_f32", "batch", "f32"), ("batch_bf16", "batch", "bf16")):
+            with Engine(mode, p, device=dev, snap=snap) as e:
+                e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+                _timed_migrate(e, w.shots[:16])                 # warm-up: autotune, graphs
+                (img, _), t = _timed_migrate(e, w.shots)
+                res[name] = len(w.shots) / t["kernel"]
+                times[name] = t
+                images[name] = img
+                tune = e.autotune_report()
+        sub = w.shots[:args.plain_shots]
+        with Engine("plain", p, device=dev) as e:
+            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+            _timed_migrate(e, sub[:2])
+            _, t = _timed_migrate(e, sub)
+            res["plain_f32"] = len(sub) / t["kernel"]
+            times["plain_f32"] = t
+        # accuracy on a 16-shot subset against an FP64 run of the same scheme
+        acc = {}
+        chk = w.shots[:16]
+        with Engine("batch", p, device=dev, arithmetic="fp64") as e:
+            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+            ref64, _ = e.migrate_f64(chk)
+        for name, mode, snap in (("batch_f32", "batch", "f32"), ("batch_bf16", "batch", "bf16"),
+                                 ("plain_f32", "plain", "f32")):
+            with Engine(mode, p, device=dev, snap=snap) as e:
+                e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+                img, _ = e.migrate(chk)
+            acc[name] = metrics.compare_images(ref64, img)["l2_relative"]
+        print(json.dumps({
+            "workload": f"config3-order{order}", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
+            "value": res["batch_bf16"], "batch_f32": res["batch_f32"], "batch_bf16": res["batch_bf16"],
+            "plain_f32": res["plain_f32"], "speedup_batch_bf16_vs_plain_f32": res["batch_bf16"] / res["plain_f32"],
+            "speedup_batch_f32_vs_plain_f32": res["batch_f32"] / res["plain_f32"],
+            "gcell_updates_per_s": {k: v["cell_updates"] / v["kernel"] / 1e9 for k, v in times.items()},
+            "rel_l2_vs_fp64": acc, "autotune": tune, "data": "synthetic (seeded model, GPU-modelled traces)",
+            "config": {"shots": len(w.shots), "plain_shots_timed": len(sub), "windows": "400-1150 columns, seed 3",
+                       "grid": f"{w.nx}x{w.nz} @{w.dx:g} m", "nt": w.nt, "order": order, "store": w.store_interval,
+                       "accuracy_subset": f"first {len(chk)} shots, FP64 GPU run of the same scheme"}}))
+        sys.stdout.flush()
+
+
+def run_config4(args):
+    """4000 x 1500 cells at 5 m, order 12, 16 shots, nt 8000: BF16 and FP16
+    snapshots with a power-of-two scale per column segment, Kahan FP32 per
+    shot, FP64 stack."""
+    import torch
+    from rtm_b200 import Engine, RTMParams, metrics, synth
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    nshots = args.shots if args.shots != SHOTS_PER_GPU else 16
+    w = synth.config4(nshots=nshots)
+    _model(w, dev)
+    p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=w.store_interval)
+    res, gc, mem = {}, {}, {}
+    for snap in ("bf16", "f16"):
+        with Engine("batch", p, device=dev, snap=snap) as e:
+            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+            mem[snap] = e.snapshot_bytes
+            (_, _), t = _timed_migrate(e, w.shots)
+            res[snap] = len(w.shots) / t["kernel"]
+            gc[snap] = t["cell_updates"] / t["kernel"] / 1e9
+    # error against FP64: FP64 snapshots of the full time axis would need
+    # 195 GB per shot, so the comparison runs 2 shots on the first 2000 steps
+    nt_chk = 2000
+    chk = w.shots[:2]
+    acc = {}
+    with Engine("batch", p, device=dev, arithmetic="fp64") as e:
+        e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=nt_chk, dt=w.dt)
+        ref64, _ = e.migrate_f64(chk)
+    for snap in ("f32", "bf16", "f16"):
+        with Engine("batch", p, device=dev, snap=snap) as e:
+            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=nt_chk, dt=w.dt)
+            img, _ = e.migrate(chk)
+        acc[snap] = metrics.compare_images(ref64, img)["l2_relative"]
+    print(json.dumps({
+        "workload": "config4", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
+        "value": res["bf16"], "bf16": res["bf16"], "f16": res["f16"], "gcell_updates_per_s": gc,
+        "snapshot_bytes_per_shot": mem, "rel_l2_vs_fp64": acc,
+        "accuracy_run": f"{len(chk)} shots, nt truncated to {nt_chk} (FP64 snapshots of the full axis: 195 GB/shot)",
+        "data": "synthetic (seeded model, GPU-modelled traces)",
+        "config": {"grid": f"{w.nx}x{w.nz} @{w.dx:g} m", "shots": len(w.shots), "nt": w.nt, "order": w.order,
+                   "store": w.store_interval}}))
+
+
+def run_config5(args):
+    """Serving stream: Poisson arrivals of migration requests with their own
+    grids (201-2000 x 151-800), orders (8/12), time axes (1400-6000) and
+    1-32 shots, admitted by snapshot memory, continuously batched."""
+    import torch
+    from rtm_b200 import Engine, RTMParams, metrics, synth
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    reqs = synth.config5_stream(nreq=args.requests, rate_hz=1.0, seed=5)
+    for r in reqs:
+        _model(r.work, dev)
+    work = sum(r.work.cell_updates() for r in reqs)
+    # arrival rate chosen so that the stream keeps the GPU about 90% busy at the
+    # throughput of the batched engine (~150 G cell updates/s)
+    busy = work / 150e9
+    gaps = np.diff([0.0] + [r.arrival for r in reqs])
+    scale = (0.9 * busy) / max(sum(gaps), 1e-9)
+    arrivals = np.cumsum(gaps * scale)
+    with Engine("serve", RTMParams(nb=60), device=dev, serve_max_nx=2000, serve_max_nz=800,
+                max_shots_in_flight=16) as e:
+        t0 = e.clock()
+        tickets, nxt, done = {}, 0, {}
+        while len(done) < len(reqs):
+            now = e.clock() - t0
+            while nxt < len(reqs) and arrivals[nxt] <= now:
+                w = reqs[nxt].work
+                tk = e.submit(w.vel, w.nx, w.nz, w.dx, w.dz, order=w.order, f0=w.f0, nt=w.nt, dt=w.dt,
+                              store_interval=w.store_interval, shots=w.shots, arrival_time=t0 + arrivals[nxt])
+                tickets[tk] = nxt
+                nxt += 1
+            e.serve_step(64)
+            for tk, i in tickets.items():
+                if i in done:
+                    continue
+                st, _, _ = e.poll(tk)
+                if st["state"] == 2:
+                    w = reqs[i].work
+                    _, img, _ = e.poll(tk, w.nx, w.nz)
+                    done[i] = (st, img)
+            if nxt < len(reqs) and not any(i not in done for i in tickets.values()):
+                time.sleep(max(0.0, min(0.05, arrivals[nxt] - (e.clock() - t0))))
+        lat = sorted(done[i][0]["finish_time"] - (t0 + arrivals[i]) for i in done)
+        span = max(done[i][0]["finish_time"] for i in done) - (t0 + arrivals[0])
+        shots = sum(len(r.work.shots) for r in reqs)
+    # accuracy of the three smallest requests against FP64 runs of the same scheme
+    acc = []
+    for i in sorted(range(len(reqs)), key=lambda k: reqs[k].work.cell_updates())[:3]:
+        w = reqs[i].work
+        with Engine("batch", RTMParams(nb=60, order=w.order, f0=w.f0, store_interval=w.store_interval), device=dev,
+                    arithmetic="fp64") as e64:
+            e64.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+            ref64, _ = e64.migrate_f64(w.shots)
+        acc.append(metrics.compare_images(ref64, done[i][1])["l2_relative"])
+    q = lambda f: lat[min(len(lat) - 1, int(f * len(lat)))]
+    print(json.dumps({
+        "workload": "config5", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
+        "value": shots / span, "latency_s": {"p50": q(0.5), "p99": q(0.99), "max": lat[-1], "min": lat[0]},
+        "gcell_updates_per_s": work / span / 1e9, "requests": len(reqs), "shots": shots,
+        "offered_load": "arrivals scaled to keep the GPU ~90% busy at 150 G cell updates/s",
+        "rel_l2_vs_fp64_smallest3": acc, "data": "synthetic (seeded models, GPU-modelled traces)",
+        "config": {"grids": "201-2000 x 151-800 @10 m", "orders": [8, 12], "nt": "1400-6000",
+                   "shots_per_request": "1-32", "seed": 5}}))
+
+
 def main():
     args = parse_args()
+    if args.impl != "reference" and args.workload != "config2":
+        {"config3": run_config3, "config4": run_config4, "config5": run_config5}[args.workload](args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

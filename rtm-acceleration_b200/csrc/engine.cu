@@ -580,6 +580,9 @@ int Engine::build_tiles() {
     RTMB_CUDA(tiles_.reserve(all.size() * sizeof(TileRef)));
     RTMB_CUDA(cudaMemcpy(tiles_.get(), all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     for (auto& g : groups_) {
+        if (!step_variant_supported(variant(g.half)))
+            return fail(RTM_B200_EUNSUPPORTED, "tile width " + std::to_string(8 * cols_) + " does not fit shared memory "
+                        "for this stencil order and precision (use tile_cols 0 or 16)");
         const int mk = g.half * 16 + cols_;
         if (!maps_.count(mk)) {
             MapPair mp;
@@ -656,15 +659,18 @@ int Engine::run_chunk(int steps) {
                 rec.key = key;
                 double best = 1e300;
                 std::pair<int, int> pick = cands[0];
+                std::map<int, int> halves;
+                for (const auto& j : jobs_)
+                    if (j.active) halves[j.m->half] = 1;
                 for (const auto& c : cands) {
                     cols_ = c.first;
                     stage_override_ = c.second;
+                    bool ok = true;   // e.g. FP64 order-12 tiles of 32 columns exceed shared memory
+                    for (const auto& h : halves) ok = ok && step_variant_supported(variant(h.first));
+                    if (!ok) { rec.us_per_step.push_back(-1.0); continue; }
                     tiles_dirty_ = true;
                     RTMB_CUDA(cudaStreamSynchronize(stream_));
                     RTMB_TRY(build_tiles());
-                    bool ok = true;
-                    for (const auto& g : groups_) ok = ok && step_variant_supported(variant(g.half));
-                    if (!ok) { rec.us_per_step.push_back(-1.0); continue; }
                     RTMB_CUDA(cudaEventRecord(tune_ev0_, stream_));
                     RTMB_TRY(run_steps(k));
                     RTMB_CUDA(cudaEventRecord(tune_ev1_, stream_));
