@@ -165,7 +165,14 @@ int rtm_b200_autotune_report(const rtm_b200_engine* h, char* buf, size_t len) {
             std::snprintf(t, sizeof t, "%s%.3f", k ? ", " : "", r.us_per_step[k]);
             js += t;
         }
-        js += "], \"cols\": " + std::to_string(r.cols) + ", \"stages\": " + std::to_string(r.stages) + "}";
+        auto choice = [](const rtmb::Engine::TuneChoice& c) {
+            return std::string("{\"kernel\": \"") + (c.kind == 1 ? "march" : "ring") + "\", \"cols\": " +
+                   std::to_string(c.cols) + ", \"stages\": " + std::to_string(c.stages) + ", \"march_m\": " +
+                   std::to_string(c.march_m) + "}";
+        };
+        js += "], \"candidates\": [";
+        for (size_t k = 0; k < r.cands.size(); ++k) js += (k ? ", " : "") + choice(r.cands[k]);
+        js += "], \"pick\": " + choice(r.pick) + "}";
     }
     js += "]";
     copy_str(js, buf, len);

@@ -119,6 +119,15 @@ int Engine::init() {
     // Failure-detection test hook: the first step launch leaves this tile's
     // stage empty, so the kernel's bounded wait must give up and report.
     if (const char* st = std::getenv("RTM_B200_STALL_TILE")) stall_tile_ = std::atoi(st);
+    // RTM_B200_STEP_KERNEL=ring|march pins the step kernel (the autotuner then
+    // only tunes that kernel's parameters); tests use it to check both kernels.
+    pin_kind_ = -1;
+    if (const char* k = std::getenv("RTM_B200_STEP_KERNEL")) {
+        if (!std::strcmp(k, "ring")) pin_kind_ = kStepRing;
+        if (!std::strcmp(k, "march")) pin_kind_ = kStepMarch;
+    }
+    if (stall_tile_ >= 0) pin_kind_ = kStepRing;   // the hook needs the ring kernel's waits
+    if (pin_kind_ >= 0) kind_ = pin_kind_;
     RTMB_CUDA(cudaEventCreate(&tune_ev0_));
     RTMB_CUDA(cudaEventCreate(&tune_ev1_));
     inited_ = true;
@@ -256,6 +265,8 @@ StepVariant Engine::variant(int half) const {
     v.half = half;
     v.cols = cols_;
     v.exact = cfg_.arithmetic == RTM_B200_ARITH_IEEE;
+    v.kind = f64_ ? kStepRing : kind_;
+    v.march_m = march_m_;
     v.nstage = step_default_stages(v);
     if (stage_override_ > 0) {
         StepVariant t = v;
@@ -539,14 +550,12 @@ int Engine::retire_finished() {
 }
 
 int Engine::build_tiles() {
-    StepVariant v;
-    v.cols = cols_;
-    const int TX = step_tile_x(v);
     std::vector<long long> sig;
     std::map<int, std::vector<TileRef>> by_half;
     for (int s = 0; s < (int)jobs_.size(); ++s) {
         const Job& j = jobs_[(size_t)s];
         if (!j.active) continue;
+        const int TX = step_tile_x(variant(j.m->half));
         const int ntx = (j.gs.nxe + TX - 1) / TX;
         std::vector<uint8_t> tflags((size_t)ntx * j.gs.ntz, 0);
         for (const auto& c : j.rec_cells) tflags[(size_t)(c.first / TX) * j.gs.ntz + c.second / kTileZ] = 1;
@@ -565,6 +574,8 @@ int Engine::build_tiles() {
     }
     sig.push_back(cols_);
     sig.push_back(stage_override_);
+    sig.push_back(kind_);
+    sig.push_back(march_m_);
     tiles_dirty_ = false;
     if (sig == tile_sig_) return RTM_B200_OK;
     tile_sig_ = sig;
@@ -584,7 +595,7 @@ int Engine::build_tiles() {
             return fail(RTM_B200_EUNSUPPORTED, "tile width " + std::to_string(8 * cols_) + " does not fit shared memory "
                         "for this stencil order and precision (use tile_cols 0 or 16)");
         const int mk = g.half * 16 + cols_;
-        if (!maps_.count(mk)) {
+        if (variant(g.half).kind == kStepRing && !maps_.count(mk)) {
             MapPair mp;
             RTMB_TRY(encode_map(g.half, true, &mp.pc));
             RTMB_TRY(encode_map(g.half, false, &mp.box));
@@ -644,30 +655,41 @@ int Engine::run_chunk(int steps) {
     if (tiles_dirty_ || groups_.empty()) {
         const std::vector<long long> key = tune_key();
         auto hit = tuned_.find(key);
-        if (hit != tuned_.end()) {
-            if (cols_ != hit->second.first || stage_override_ != hit->second.second) {
-                cols_ = hit->second.first;
-                stage_override_ = hit->second.second;
+        auto apply = [&](const TuneChoice& c) {
+            if (kind_ != c.kind || cols_ != c.cols || stage_override_ != c.stages || march_m_ != c.march_m)
                 tiles_dirty_ = true;
-            }
+            kind_ = c.kind;
+            cols_ = c.cols;
+            stage_override_ = c.stages;
+            march_m_ = c.march_m;
+        };
+        if (hit != tuned_.end()) {
+            apply(hit->second);
         } else {
-            const std::pair<int, int> cands[] = {{2, 0}, {2, 2}, {4, 0}, {4, 3}};
-            const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
-            const int k = std::min(16, steps / ncand);
+            std::vector<TuneChoice> cands = {{kStepRing, 2, 0, 3}, {kStepRing, 2, 2, 3}, {kStepRing, 4, 0, 3},
+                                             {kStepMarch, 2, 0, 2}, {kStepMarch, 2, 0, 3}, {kStepMarch, 2, 0, 5}};
+            if (pin_kind_ >= 0) {
+                std::vector<TuneChoice> keep;
+                for (const auto& c : cands)
+                    if (c.kind == pin_kind_) keep.push_back(c);
+                cands.swap(keep);
+            }
+            const int ncand = (int)cands.size();
+            const int k = std::min(16, steps / std::max(ncand, 1));
             if (k >= 4) {
                 TuneRecord rec;
                 rec.key = key;
                 double best = 1e300;
-                std::pair<int, int> pick = cands[0];
+                TuneChoice pick = cands[0];
                 std::map<int, int> halves;
                 for (const auto& j : jobs_)
                     if (j.active) halves[j.m->half] = 1;
                 for (const auto& c : cands) {
-                    cols_ = c.first;
-                    stage_override_ = c.second;
+                    apply(c);
+                    rec.cands.push_back(c);
                     bool ok = true;   // e.g. FP64 order-12 tiles of 32 columns exceed shared memory
                     for (const auto& h : halves) ok = ok && step_variant_supported(variant(h.first));
-                    if (!ok) { rec.us_per_step.push_back(-1.0); continue; }
+                    if (!ok || (f64_ && c.kind == kStepMarch)) { rec.us_per_step.push_back(-1.0); continue; }
                     tiles_dirty_ = true;
                     RTMB_CUDA(cudaStreamSynchronize(stream_));
                     RTMB_TRY(build_tiles());
@@ -682,10 +704,8 @@ int Engine::run_chunk(int steps) {
                     if (us < best) { best = us; pick = c; }
                     steps -= k;
                 }
-                cols_ = pick.first;
-                stage_override_ = pick.second;
-                rec.cols = pick.first;
-                rec.stages = pick.second;
+                apply(pick);
+                rec.pick = pick;
                 tuned_[key] = pick;
                 tune_log_.push_back(rec);
                 tiles_dirty_ = true;
@@ -719,7 +739,9 @@ int Engine::run_steps(int steps) {
                     p.stall_tile = stall_tile_;
                     stall_tile_ = -1;
                 }
-                const MapPair& mp = maps_[g.half * 16 + cols_];
+                p.march_m = v.march_m;
+                static const MapPair kNoMaps{};
+                const MapPair& mp = v.kind == kStepRing ? maps_[g.half * 16 + cols_] : kNoMaps;
                 RTMB_CUDA(launch_step(v, mp.pc, mp.box, p, stream_));
             }
         RTMB_CUDA(launch_advance_counter(counter_.get<long long>(), steps, stream_));

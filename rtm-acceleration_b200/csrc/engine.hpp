@@ -199,18 +199,29 @@ private:
     std::vector<long long> graph_sig_;
     int graph_steps_ = 0;
     int launches_ = 0;
-    int cols_ = 4;
-    int stage_override_ = 0;
-    int stall_tile_ = -1;                    // failure-detection test hook (RTM_B200_STALL_TILE)                 // pipeline stages chosen by the autotuner (0 = default)
-    // Autotuner: the fastest (columns per warp, pipeline stages) measured on
-    // real steps, cached per job mix (stencil orders, tile rows, shots in flight).
+    int cols_ = 4;                           // ring kernel: columns per consumer warp
+    int stage_override_ = 0;                 // ring kernel: pipeline stages (0 = default)
+    int stall_tile_ = -1;                    // failure-detection test hook (RTM_B200_STALL_TILE)
+    // Autotuner: the fastest step kernel and parameters measured on real steps,
+    // cached per job mix (stencil orders, tile rows, shots in flight).
     bool autotune_ = false;
-    std::map<std::vector<long long>, std::pair<int, int>> tuned_;
+    int kind_ = 0;                           // kStepRing or kStepMarch (autotuned)
+    int march_m_ = 3;                        // march strip length, units of 2H+1 columns
+    int pin_kind_ = -1;                      // step kernel pinned by RTM_B200_STEP_KERNEL (-1: tuned)
+public:
+    struct TuneChoice { int kind, cols, stages, march_m; };
+private:
+    std::map<std::vector<long long>, TuneChoice> tuned_;
     std::vector<long long> tune_key() const;
     int run_steps(int steps);
     cudaEvent_t tune_ev0_ = nullptr, tune_ev1_ = nullptr;
 public:
-    struct TuneRecord { std::vector<long long> key; int cols, stages; std::vector<double> us_per_step; };
+    struct TuneRecord {
+        std::vector<long long> key;
+        TuneChoice pick;
+        std::vector<TuneChoice> cands;
+        std::vector<double> us_per_step;
+    };
     std::vector<TuneRecord> tune_log_;
 private:
     // backpressure: at most kChunksInFlight chunks queued ahead of the GPU

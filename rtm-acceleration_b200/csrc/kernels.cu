@@ -119,8 +119,56 @@ cudaError_t attr_by_half(int half) {
 
 }  // namespace
 
+// ----------------------------------------------------------- march kernel
+template <int H, bool EX>
+int march_grid_impl() {
+    static std::once_flag once;
+    static int grid = 0;
+    std::call_once(once, [] {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, march_kernel<H, EX>, kMarchThreads, 0) ==
+                cudaSuccess && per > 0)
+            grid = sms * per;
+    });
+    return grid;
+}
+
+template <int H, bool EX>
+cudaError_t march_launch_impl(const StepParams& p, cudaStream_t s) {
+    const int cap = march_grid_impl<H, EX>();
+    if (cap <= 0) return cudaErrorInvalidConfiguration;
+    const int want = (p.ntiles + kMarchWarps - 1) / kMarchWarps;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(want < cap ? want : cap));
+    cfg.blockDim = dim3(kMarchThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p.pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, march_kernel<H, EX>, p);
+}
+
+template <bool EX>
+cudaError_t march_by_half(int half, const StepParams& p, cudaStream_t s) {
+    switch (half) {
+        case 1: return march_launch_impl<1, EX>(p, s);
+        case 2: return march_launch_impl<2, EX>(p, s);
+        case 3: return march_launch_impl<3, EX>(p, s);
+        case 4: return march_launch_impl<4, EX>(p, s);
+        case 5: return march_launch_impl<5, EX>(p, s);
+        case 6: return march_launch_impl<6, EX>(p, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t prepare_step(const StepVariant& v) {
     if (!step_variant_supported(v)) return cudaErrorInvalidValue;
+    if (v.kind == kStepMarch) return cudaSuccess;
     if (step_max_grid(v) <= 0) return cudaErrorInvalidValue;
     if (v.f64) return v.cols == 4 ? attr_by_half<double, false, 4>(v.half) : attr_by_half<double, false, 2>(v.half);
     if (v.exact) return v.cols == 4 ? attr_by_half<float, true, 4>(v.half) : attr_by_half<float, true, 2>(v.half);
@@ -129,6 +177,8 @@ cudaError_t prepare_step(const StepVariant& v) {
 
 bool step_variant_supported(const StepVariant& v) {
     if (v.half < 1 || v.half > kMaxHalf) return false;
+    if (v.kind == kStepMarch) return !v.f64 && v.march_m >= 1 && v.march_m <= 9;
+    if (v.kind != kStepRing) return false;
     if (v.cols != 2 && v.cols != 4) return false;
     if (v.nstage < 2 || v.nstage > kMaxStages) return false;
     return step_smem_bytes(v) <= 227 * 1024;
@@ -163,6 +213,7 @@ int step_default_stages(const StepVariant& v) {
 
 int step_max_grid(const StepVariant& v) {
     if (!step_variant_supported(v)) return 0;
+    if (v.kind == kStepMarch) return 1;
     if (v.f64)
         return v.cols == 4 ? grid_by_half<double, false, 4>(v.half, v.nstage)
                            : grid_by_half<double, false, 2>(v.half, v.nstage);
@@ -178,6 +229,8 @@ cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUte
     if (!step_variant_supported(v) || pin.ntiles <= 0) return cudaErrorInvalidValue;
     StepParams p = pin;
     p.nstage = v.nstage;
+    p.march_m = v.march_m;
+    if (v.kind == kStepMarch) return v.exact ? march_by_half<true>(v.half, p, s) : march_by_half<false>(v.half, p, s);
     if (v.f64) {
         if (v.cols == 4) return by_half<double, false, 4>(v.half, mpc, mpp, p, s);
         return by_half<double, false, 2>(v.half, mpc, mpp, p, s);

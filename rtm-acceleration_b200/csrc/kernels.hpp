@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "internal.hpp"
+#include "march_kernel.cuh"
 #include "step_kernel.cuh"
 
 namespace rtmb {
@@ -15,12 +16,19 @@ struct StepVariant {
     bool exact = true;  // IEEE unfused float arithmetic (bit-identical path)
     int cols = 4;       // columns per consumer warp; tile is 128 rows x (8*cols) columns
     int nstage = 3;     // shared-memory pipeline stages, 2..kMaxStages
+    int kind = 0;       // 0: TMA ring kernel (step_kernel); 1: register march (march_kernel, FP32)
+    int march_m = 3;    // march: strip length in units of 2*half+1 columns (1..9)
 };
+
+constexpr int kStepRing = 0;
+constexpr int kStepMarch = 1;
 
 constexpr int kStepWarps = 8;                        // consumer warps
 constexpr int kStepThreads = (kStepWarps + 1) * 32;  // + the producer warp
 
-inline int step_tile_x(const StepVariant& v) { return kStepWarps * v.cols; }
+inline int step_tile_x(const StepVariant& v) {
+    return v.kind == kStepMarch ? (2 * v.half + 1) * v.march_m : kStepWarps * v.cols;
+}
 inline int step_halo_rows(const StepVariant& v) { return (v.half + 3) & ~3; }
 inline int step_box_z(const StepVariant& v) { return kTileZ + 2 * step_halo_rows(v); }
 inline int step_box_x(const StepVariant& v) { return step_tile_x(v) + 2 * v.half; }

@@ -57,6 +57,7 @@ struct StepParams {
     int nstage;                     // pipeline stages (2..4) in dynamic shared memory
     int pdl;                        // host side: launch as a programmatic dependent launch
     int stall_tile;                 // failure-detection test: this tile is never produced (-1: none)
+    int march_m;                    // march kernel: strip length in units of 2H+1 columns
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -603,6 +604,63 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parit
     return true;
 }
 
+// What a tile does at global step g (identical in every lane): active,
+// forward or backward pass, time index, first step of the pass, which field
+// level holds p^n, stored step, receiver work.  rec_staged is filled later.
+__device__ __forceinline__ TileInfo decode_tile(const TileRef& tr, long long g) {
+    TileInfo ti{};
+    const long long n = g - tr.g0;
+    ti.active = n >= 0 && n < tr.total_steps;
+    if (!ti.active) return ti;
+    const int nt = tr.nt;
+    ti.fwd = n < nt;
+    const int j = ti.fwd ? (int)n : (int)(n - nt);
+    ti.it = ti.fwd ? j : nt - 1 - j;
+    ti.first = j == 0;
+    ti.cur = j & 1;
+    ti.x0 = tr.x0;
+    ti.z0 = tr.z0;
+    ti.tz = tr.tz;
+    const int ks = ti.it / tr.si;
+    const bool stored = ks * tr.si == ti.it;
+    ti.do_snap = ti.fwd && stored && (tr.flags & kFlagSnapshots);
+    ti.do_image = !ti.fwd && stored && (tr.flags & kFlagImage);
+    ti.ksnap = ks;
+    const bool pts_matter = !ti.fwd || (tr.flags & kFlagRecord);
+    ti.has_pts = pts_matter && tr.has_pts;
+    return ti;
+}
+
+// Stages the receivers of columns [x0, x0 + ncols) into re[] with per-column
+// offsets rcs[0..ncols] (warp-cooperative).  Returns false, staging nothing,
+// when the columns hold more than kTileRec receivers.
+__device__ __forceinline__ bool stage_receivers(const ShotDesc& gd, const TileInfo& ti, int x0, int ncols, int nxe,
+                                                int* rcs, RecEntry* re) {
+    const int lane = threadIdx.x & 31;
+    const int* rec_col = gd.rec_col;
+    if (!rec_col) return false;
+    const int xe = x0 + ncols < nxe ? x0 + ncols : nxe;
+    const int r_lo = __ldg(rec_col + x0);
+    const int nrec = __ldg(rec_col + xe) - r_lo;
+    if (nrec > kTileRec) return false;
+    for (int k = lane; k <= ncols; k += 32) {
+        const int x = x0 + k < nxe ? x0 + k : nxe;
+        rcs[k] = __ldg(rec_col + x) - r_lo;
+    }
+    const int* pts_ir = gd.pts_ir;
+    const int* rec_zs = gd.rec_zs;
+    const float* traces = gd.traces;
+    const int trace_nt = gd.trace_nt;
+    for (int k = lane; k < nrec; k += 32) {
+        RecEntry e;
+        e.ir = __ldg(pts_ir + r_lo + k);
+        e.z = __ldg(rec_zs + r_lo + k);
+        e.tr = ti.fwd ? 0.f : __ldg(traces + (size_t)e.ir * trace_nt + ti.it);
+        re[k] = e;
+    }
+    return true;
+}
+
 // Fills one stage with tile `t` (producer warp, all 32 lanes).  Lane 0 decodes
 // what the tile does this step and publishes it as TileInfo; the lanes copy
 // the shot descriptor, the tile's taper weights and (for tiles with receiver
@@ -620,30 +678,12 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
     const int lane = threadIdx.x & 31;
     // Decode the step (every lane, identically) and issue the boxes first: they
     // depend on the TileRef only.
-    TileInfo ti{};
-    const long long n = g - tr.g0;
-    ti.active = n >= 0 && n < tr.total_steps;
+    const TileInfo ti = decode_tile(tr, g);
     if (!ti.active) {
         if (lane == 0) *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
         mbar_arrive(full);
         return;
     }
-    const int nt = tr.nt;
-    ti.fwd = n < nt;
-    const int j = ti.fwd ? (int)n : (int)(n - nt);
-    ti.it = ti.fwd ? j : nt - 1 - j;
-    ti.first = j == 0;
-    ti.cur = j & 1;
-    ti.x0 = tr.x0;
-    ti.z0 = tr.z0;
-    ti.tz = tr.tz;
-    const int ks = ti.it / tr.si;
-    const bool stored = ks * tr.si == ti.it;
-    ti.do_snap = ti.fwd && stored && (tr.flags & kFlagSnapshots);
-    ti.do_image = !ti.fwd && stored && (tr.flags & kFlagImage);
-    ti.ksnap = ks;
-    const bool pts_matter = !ti.fwd || (tr.flags & kFlagRecord);
-    ti.has_pts = pts_matter && tr.has_pts;
     const int x0 = tr.x0, z0 = tr.z0;
     if (lane == 0) {
         *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
@@ -678,39 +718,14 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
         // Stage the tile's receivers (row, index and, backward, this step's
         // trace sample) so consumers never chase the receiver lists in global
         // memory; a tile with more than kTileRec receivers keeps the global path.
-        int staged = 0;
-        const int* rec_col = gd.rec_col;
-        if (rec_col) {
-            const int xe = x0 + S::TX < nxe ? x0 + S::TX : nxe;
-            const int r_lo = __ldg(rec_col + x0);
-            const int nrec = __ldg(rec_col + xe) - r_lo;
-            if (nrec <= kTileRec) {
-                staged = 1;
-                int* rcs = reinterpret_cast<int*>(st + S::RCS_OFF);
-                for (int k = lane; k <= S::TX; k += 32) {
-                    const int x = x0 + k < nxe ? x0 + k : nxe;
-                    rcs[k] = __ldg(rec_col + x) - r_lo;
-                }
-                const int* pts_ir = gd.pts_ir;
-                const int* rec_zs = gd.rec_zs;
-                const float* traces = gd.traces;
-                const int trace_nt = gd.trace_nt;
-                RecEntry* re = reinterpret_cast<RecEntry*>(st + S::REC_OFF);
-                for (int k = lane; k < nrec; k += 32) {
-                    RecEntry e;
-                    e.ir = __ldg(pts_ir + r_lo + k);
-                    e.z = __ldg(rec_zs + r_lo + k);
-                    e.tr = ti.fwd ? 0.f : __ldg(traces + (size_t)e.ir * trace_nt + ti.it);
-                    re[k] = e;
-                }
-            }
-        }
+        const bool staged = stage_receivers(gd, ti, x0, S::TX, nxe, reinterpret_cast<int*>(st + S::RCS_OFF),
+                                            reinterpret_cast<RecEntry*>(st + S::REC_OFF));
         if (!staged)
             for (int k = lane; k <= S::TX; k += 32) {
                 const int x = x0 + k < nxe ? x0 + k : nxe;
                 reinterpret_cast<int*>(st + S::CS_OFF)[k] = __ldg(gd.col_start + x);
             }
-        if (lane == 0) reinterpret_cast<TileInfo*>(st + S::INFO_OFF)->rec_staged = staged;
+        if (lane == 0) reinterpret_cast<TileInfo*>(st + S::INFO_OFF)->rec_staged = staged ? 1 : 0;
     }
     // Stored backward steps: pull the tile's snapshot lines into L2 now, so the
     // consumers' snapshot loads a few tiles later hit L2 instead of HBM.
