@@ -6,7 +6,7 @@
  * Each entry point replaces one member of the reference's engine interface
  * (Marouane-Djabri/RTM-Acceleration, include/rtm_engine.hpp and
  * include/rtm_factory.hpp); the citation is given beside each declaration.  The
- * C++ class rtm::B200RTM (include/rtm_engine.hpp of this repository) wraps these
+ * C++ class rtm_b200::B200RTM (include/rtm_b200_engine.hpp of this repository) wraps these
  * calls into the reference's RTMEngine interface and throws std::runtime_error
  * on a non-zero status, like the reference.
  *
