@@ -177,6 +177,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// The same test, but a thread whose phase is not complete is suspended (it
+// issues nothing) until the phase completes or about `hint_ns` pass, so a
+// waiting warp leaves the issue slots to the warps that have work.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+constexpr uint32_t kSleepHintNs = 20000;
 // Plain (non-multicast) tiled TMA load of a 3D box from this GPU's own memory.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
                                             int c2) {
@@ -591,9 +606,9 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 // Bounded wait that also gives up as soon as another warp of the CTA aborted.
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                                    int* err) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_sleep(bar, parity, kSleepHintNs)) return true;
     const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait(bar, parity)) {
+    while (!mbar_try_wait_sleep(bar, parity, kSleepHintNs)) {
         if (*abort_flag) return false;
         if (global_ns() - t0 > kWaitNs) {
             atomicOr(err, kErrTmaTimeout);
