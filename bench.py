@@ -341,6 +341,7 @@ def run_b200_arm(args):
         rel64 = metrics.compare_images(ref64, img_h)["l2_relative"]
 
     l2_gbs = eng.memory_probe(48 << 20, 50)
+    tune = [r["pick"] for r in eng.autotune_report()]
     eng.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -372,7 +373,7 @@ def run_b200_arm(args):
                                f"order {w.order}, store {w.store_interval}",
                    "engine": args.mode, "max_shots_in_flight": args.max_in_flight, "tile_cols": args.tile_cols,
                    "snapshots": args.snap, "arithmetic": args.arith, "accumulation": "compensated FP32 + FP64 stack",
-                   "l2": "inputs and snapshots larger than L2 (126 MB)"},
+                   "l2": "inputs and snapshots larger than L2 (126 MB)", "autotuned_step_kernel": tune},
         "gcell_updates_per_s": gcell,
         "rel_l2_vs_fp64": rel64,
         "gpu_launches": launches,

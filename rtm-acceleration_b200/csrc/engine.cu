@@ -674,35 +674,44 @@ int Engine::run_chunk(int steps) {
                     if (c.kind == pin_kind_) keep.push_back(c);
                 cands.swap(keep);
             }
+            // Two interleaved rounds of k timed steps per candidate; a
+            // candidate's time is its faster round, so one disturbed sample
+            // cannot decide the pick.
             const int ncand = (int)cands.size();
-            const int k = std::min(16, steps / std::max(ncand, 1));
+            const int k = std::min(12, steps / std::max(2 * ncand, 1));
             if (k >= 4) {
                 TuneRecord rec;
                 rec.key = key;
-                double best = 1e300;
-                TuneChoice pick = cands[0];
                 std::map<int, int> halves;
                 for (const auto& j : jobs_)
                     if (j.active) halves[j.m->half] = 1;
-                for (const auto& c : cands) {
-                    apply(c);
-                    rec.cands.push_back(c);
-                    bool ok = true;   // e.g. FP64 order-12 tiles of 32 columns exceed shared memory
-                    for (const auto& h : halves) ok = ok && step_variant_supported(variant(h.first));
-                    if (!ok || (f64_ && c.kind == kStepMarch)) { rec.us_per_step.push_back(-1.0); continue; }
-                    tiles_dirty_ = true;
-                    RTMB_CUDA(cudaStreamSynchronize(stream_));
-                    RTMB_TRY(build_tiles());
-                    RTMB_CUDA(cudaEventRecord(tune_ev0_, stream_));
-                    RTMB_TRY(run_steps(k));
-                    RTMB_CUDA(cudaEventRecord(tune_ev1_, stream_));
-                    RTMB_CUDA(cudaEventSynchronize(tune_ev1_));
-                    float ms = 0.f;
-                    RTMB_CUDA(cudaEventElapsedTime(&ms, tune_ev0_, tune_ev1_));
-                    const double us = 1e3 * ms / k;
+                std::vector<double> best_us((size_t)ncand, 1e300);
+                for (int round = 0; round < 2; ++round)
+                    for (int ci = 0; ci < ncand; ++ci) {
+                        const TuneChoice& c = cands[(size_t)ci];
+                        apply(c);
+                        bool ok = true;   // e.g. FP64 order-12 tiles of 32 columns exceed shared memory
+                        for (const auto& h : halves) ok = ok && step_variant_supported(variant(h.first));
+                        if (!ok || (f64_ && c.kind == kStepMarch)) continue;
+                        tiles_dirty_ = true;
+                        RTMB_CUDA(cudaStreamSynchronize(stream_));
+                        RTMB_TRY(build_tiles());
+                        RTMB_CUDA(cudaEventRecord(tune_ev0_, stream_));
+                        RTMB_TRY(run_steps(k));
+                        RTMB_CUDA(cudaEventRecord(tune_ev1_, stream_));
+                        RTMB_CUDA(cudaEventSynchronize(tune_ev1_));
+                        float ms = 0.f;
+                        RTMB_CUDA(cudaEventElapsedTime(&ms, tune_ev0_, tune_ev1_));
+                        best_us[(size_t)ci] = std::min(best_us[(size_t)ci], 1e3 * ms / k);
+                        steps -= k;
+                    }
+                TuneChoice pick = cands[0];
+                double best = 1e300;
+                for (int ci = 0; ci < ncand; ++ci) {
+                    rec.cands.push_back(cands[(size_t)ci]);
+                    const double us = best_us[(size_t)ci] < 1e299 ? best_us[(size_t)ci] : -1.0;
                     rec.us_per_step.push_back(us);
-                    if (us < best) { best = us; pick = c; }
-                    steps -= k;
+                    if (us > 0 && us < best) { best = us; pick = cands[(size_t)ci]; }
                 }
                 apply(pick);
                 rec.pick = pick;
