@@ -65,7 +65,7 @@ def parse_args():
     ap.add_argument("--arith", default="ieee", choices=["ieee", "fma"])
     ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
+    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
                     help="config2 is the contract line; the others print one extra JSON line each")
     ap.add_argument("--plain-shots", type=int, default=64, help="config3: shots timed on the plain engine")
     ap.add_argument("--requests", type=int, default=24, help="config5: requests in the stream")
@@ -408,6 +408,63 @@ def _model(w, device, shots=None):
         s.traces = t
 
 
+def run_config1(args):
+    """The reference's CPU-runnable case (201 x 151, 3 flat layers, 4 shots,
+    nt 1400, order 8, store 2, direct-wave mute 1500 m/s): the plain engine
+    (bit-identical to the reference) and the batched engine against the
+    reference's own cpu and cpu-opt engines on this host, same files."""
+    import torch
+    from rtm_b200 import Engine, RTMParams, metrics, mute_direct_wave, synth
+    from rtm_b200 import io as rio
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    w = synth.config1(dipping=False)
+    _model(w, dev)
+    t_pad = float(np.float32(1.0) / np.float32(w.f0))
+    for sh in w.shots:
+        mute_direct_wave(sh, w.mute_v, t_pad, t_pad)
+    p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=w.store_interval)
+    res, imgs = {}, {}
+    for name, mode in (("plain", "plain"), ("batch", "batch")):
+        with Engine(mode, p, device=dev) as e:
+            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+            _timed_migrate(e, w.shots)
+            (img, _), t = _timed_migrate(e, w.shots)
+            res[name] = {"shots_per_s": len(w.shots) / t["kernel"], "gcell_updates_per_s":
+                         t["cell_updates"] / t["kernel"] / 1e9, "seconds": t["kernel"]}
+            imgs[name] = img
+    cpu = {}
+    ref = os.path.join(ROOT, "oracle", "_ref", "rtm")
+    if os.path.exists(ref):
+        with tempfile.TemporaryDirectory() as td:
+            vel = os.path.join(td, "v.bin")
+            rio.write_velocity_raw(vel, w.vel)
+            rio.write_header_file(vel + ".hdr", rio.VelocityHeader(w.nx, w.nz, w.dx, w.dz, 0.0, 0.0, "zfast"))
+            shp = os.path.join(td, "s.bin")
+            # the unmuted traces: the reference applies the mute itself
+            raw = synth.config1(dipping=False)
+            _model(raw, dev)
+            rio.write_shots_raw(shp, raw.shots)
+            for eng, threads in (("cpu", 1), ("cpu-opt", os.cpu_count() or 1)):
+                out = os.path.join(td, f"{eng}.bin")
+                t0 = time.perf_counter()
+                subprocess.run([ref, "--engine", eng, "--velocity", vel, "--shots", shp, "--output", out,
+                                "--order", "8", "--nb", "60", "--f0", "12", "--store-interval", "2",
+                                "--mute-direct", "1500", "--quiet"], check=True, stdout=subprocess.DEVNULL,
+                               env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+                sec = time.perf_counter() - t0
+                ref_img = rio.read_raw_floats(out)
+                cpu[eng] = {"shots_per_s": len(w.shots) / sec, "seconds_wall": sec, "threads": threads,
+                            "plain_bit_identical": bool(np.array_equal(ref_img.view(np.uint32),
+                                                                       imgs["plain"].view(np.uint32))),
+                            "batch_rel_l2": metrics.compare_images(ref_img, imgs["batch"])["l2_relative"]}
+    print(json.dumps({"workload": "config1", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
+                      "value": res["plain"]["shots_per_s"], "b200": res, "reference_cpu": cpu,
+                      "data": "synthetic (the reference's generator recipe, GPU-modelled traces)",
+                      "config": {"grid": "201x151 @10 m", "shots": 4, "nt": 1400, "order": 8, "store": 2,
+                                 "mute": 1500}}))
+
+
 def run_config3(args):
     """256 shots on uneven aperture windows (400-1150 columns of the
     1150 x 400 model), orders 8 and 12: the batched engine (FP32 and BF16
@@ -573,7 +630,8 @@ def run_config5(args):
 def main():
     args = parse_args()
     if args.impl != "reference" and args.workload != "config2":
-        {"config3": run_config3, "config4": run_config4, "config5": run_config5}[args.workload](args)
+        {"config1": run_config1, "config3": run_config3, "config4": run_config4,
+         "config5": run_config5}[args.workload](args)
         return
     if args.impl == "reference":
         run_reference_arm(args)

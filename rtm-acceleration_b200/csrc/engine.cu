@@ -409,7 +409,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     ShotDesc d{};
     d.nxe = gs.nxe; d.nze = gs.nze; d.nx = gs.nx; d.nz = gs.nz; d.nb = gs.nb;
     d.model_x0 = sh.x0; d.win_nx = gs.nx;
-    d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz; d.ntx = 0;   // tiles are listed per tile width (autotuned)
+    d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz;
     d.nt = m->nt; d.si = m->si; d.nsnap = m->nsnap;
     job.first_phase_step = backward_only == 1 ? m->nt : 0;
     job.g0 = g_ - job.first_phase_step;
@@ -430,7 +430,6 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     d.wavelet = m->wavelet.get<float>();
     d.traces = dev_traces ? sh.traces : sl.traces.get<float>();
     d.col_start = sl.col_start.get<int>();
-    d.tile_pts = nullptr;
     d.pts = sl.pts.get<PointEntry>();
     d.pts_ir = sl.ir.get<int>();
     d.rec_col = sl.rec_col.get<int>();

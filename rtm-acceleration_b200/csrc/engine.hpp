@@ -84,7 +84,7 @@ struct Job {
 };
 
 struct Slot {
-    DevMem wx, col_start, pts, ir, rec_col, rec_z, traces, rec, acc, tile_pts;
+    DevMem wx, col_start, pts, ir, rec_col, rec_z, traces, rec, acc;
     PinnedMem stage;
     cudaEvent_t staged = nullptr;      // H2D from `stage` finished
 };

@@ -53,8 +53,8 @@ struct ShotDesc {
     int model_x0;        // first model column of this shot's aperture window
     int win_nx;          // window width in model columns (== nx)
     int zs0, lds;        // snapshot/image row origin (extended z) and pitch
-    int ntz;             // tiles in z (scale-exponent stride)
-    int ntx;             // unused (tiles in x depend on the tuned tile width)
+    int ntz;             // 128-row bands (stride of the snapshot scale exponents)
+    int pad1;
     // time
     int nt, si, nsnap;
     long long g0;        // global step at which forward step 0 runs
@@ -77,7 +77,6 @@ struct ShotDesc {
     const float* wavelet;    // nt
     const float* traces;     // nrec * trace_nt, trace-major
     const int* col_start;    // nxe+1 offsets into pts
-    const uint8_t* tile_pts; // unused (TileRef.has_pts marks receiver tiles)
     const PointEntry* pts;
     const int* pts_ir;
     const int* rec_col;      // nxe+1 receiver offsets per column (null: not staged)

@@ -156,7 +156,6 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     const size_t o_cs = take(geo.col_start.size() * 4);
     const size_t o_pts = take(std::max<size_t>(geo.pts.size(), 1) * sizeof(PointEntry));
     const size_t o_ir = take(std::max<size_t>(geo.ir.size(), 1) * 4);
-    const size_t o_tf = take(tflags.size());
     const size_t o_desc = take(sizeof(ShotDesc));
     const size_t o_tiles = take(ntiles * sizeof(TileRef));
     const size_t o_ctr = take(sizeof(long long) + sizeof(int));
@@ -185,7 +184,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
 
     ShotDesc d{};
     d.nxe = g.nxe; d.nze = g.nze; d.nx = g.nx; d.nz = g.nz; d.nb = g.nb;
-    d.model_x0 = 0; d.win_nx = g.nx; d.zs0 = g.zs0; d.lds = g.lds; d.ntz = g.ntz; d.ntx = ntx;
+    d.model_x0 = 0; d.win_nx = g.nx; d.zs0 = g.zs0; d.lds = g.lds; d.ntz = g.ntz;
     d.nt = pr->nt; d.si = 1; d.nsnap = pr->nt;
     d.g0 = 0; d.total_steps = pr->nt; d.trace_nt = pr->nt;
     d.src_x = geo.src_x; d.src_z = geo.src_z;
@@ -201,7 +200,6 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     d.wz = reinterpret_cast<const float*>(base + o_wz);
     d.wavelet = reinterpret_cast<const float*>(base + o_wav);
     d.col_start = reinterpret_cast<const int*>(base + o_cs);
-    d.tile_pts = reinterpret_cast<const uint8_t*>(base + o_tf);
     d.pts = reinterpret_cast<const PointEntry*>(base + o_pts);
     d.pts_ir = reinterpret_cast<const int*>(base + o_ir);
     d.rec_out = out_on_device ? traces_out : reinterpret_cast<float*>(base + o_rec);
@@ -215,7 +213,6 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     if (!geo.pts.empty())
         SS_CUDA(cudaMemcpy(base + o_pts, geo.pts.data(), geo.pts.size() * sizeof(PointEntry), cudaMemcpyHostToDevice));
     if (!geo.ir.empty()) SS_CUDA(cudaMemcpy(base + o_ir, geo.ir.data(), geo.ir.size() * 4, cudaMemcpyHostToDevice));
-    SS_CUDA(cudaMemcpy(base + o_tf, tflags.data(), tflags.size(), cudaMemcpyHostToDevice));
     SS_CUDA(cudaMemcpy(base + o_desc, &d, sizeof(ShotDesc), cudaMemcpyHostToDevice));
     std::vector<TileRef> tiles;
     tiles.reserve(ntiles);
