@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kMarchThreads) march_kernel(const StepParams p
                     }
                 }
                 column_epilogue<T, H, EXACT>(d, ti, x, zr, lane, lane_in, lane_snap, val, vd, fs, Iv, Sv, rkb, rke,
-                                             W.re, pc_buf, pn_buf, ldz);
+                                             W.re, pc_buf, pn_buf, ldz, 32);
             }
         }
     }

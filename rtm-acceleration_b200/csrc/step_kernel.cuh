@@ -361,7 +361,7 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
                                                 bool lane_in, bool lane_snap, T (&val)[4], const T (&vd)[4],
                                                 const T (&fs)[4], T (&Iv)[4], T (&Sv)[4], int rkb, int rke,
                                                 const RecEntry* __restrict__ re, T* __restrict__ pcur,
-                                                T* __restrict__ pnext, int ldz) {
+                                                T* __restrict__ pnext, int ldz, int G) {
     using A = Arith<T, EXACT>;
     const int nxe = d.nxe, nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
     const int it = t.it;
@@ -431,19 +431,28 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
         }
     }
 
+    // Power-of-two scale of a reduced-precision snapshot, one per (snapshot,
+    // column, 128-row segment): the maximum over the G lanes of the column,
+    // taken by every lane of the warp (the shuffles need all 32).
+    float amax_col = 0.f;
+    if (do_snap && (snap_type == kSnapBF16 || snap_type == kSnapF16)) {
+        float a = 0.f;
+        if (col_int && lane_snap)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a = fmaxf(a, fabsf((float)val[q]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            if (o < G) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+        amax_col = a;
+    }
+
     if (col_int && (do_snap || do_image)) {
         if (do_snap) {
             const size_t cell = (size_t)t.ksnap * nx * lds + ic;
             if (snap_type == kSnapF32 || snap_type == kSnapF64) {
                 if (lane_snap) stg4cs(reinterpret_cast<T*>(d.snap) + cell, val);
             } else {
-                // power-of-two scale per (snapshot, column, 128-row segment)
-                float amax = 0.f;
-                if (lane_snap)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) amax = fmaxf(amax, fabsf((float)val[q]));
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+                const float amax = amax_col;
                 int e = 0;
                 if (amax > 0.f) {
                     // amax <= 2^e from the exponent field (subnormals: e = -126)
@@ -453,7 +462,7 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
                     e = e < -126 ? -126 : (e > 127 ? 127 : e);
                 }
                 const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
-                if (lane == 0) d.snap_exp[eidx] = (int8_t)e;
+                if ((lane & (G - 1)) == 0) d.snap_exp[eidx] = (int8_t)e;
                 if (lane_snap) {
                     const float inv = pow2f(-e);
                     uint2 packed;
@@ -525,11 +534,24 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int zr = t.z0 + 4 * lane;              // first of this thread's 4 rows
     const int nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
     const bool first = t.first;
-    const bool lane_in = zr < nze;
     const bool do_image = t.do_image;
+
+    // A band with few live rows (the last band of a shot) packs several columns
+    // into one warp: G lanes per column (the fewest float4 lanes that cover the
+    // live rows, a power of two, and at least 32 / TX) and 32 / G columns per
+    // pass.  Passes go round-robin over the warps from a first warp that moves
+    // with the tile's x position, so that the packed bands of successive tiles
+    // land on different warps.  G = 32 is one column per pass.
+    const int live = nze - t.z0 < kTileZ ? nze - t.z0 : kTileZ;
+    int G = 32;
+    while (G > 1 && 4 * (G / 2) >= live && 32 / (G / 2) <= S::TX) G >>= 1;
+    const int cpp = 32 / G;
+    const int sub = lane & (G - 1);              // this thread's float4 slot in the column
+    const int zr = t.z0 + 4 * sub;               // first of this thread's 4 rows
+    const bool lane_in = zr < nze;
+    const bool lane_snap = lane_in && zr >= zs0 && zr < zs0 + lds;
 
     const T c0 = (T)d.c0;
     const float* cx = d.cx;     // read from shared memory where used
@@ -537,16 +559,17 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
 
     float wz[4];
     {
-        const float4 w4 = *reinterpret_cast<const float4*>(sm_wz + 4 * lane);
+        const float4 w4 = *reinterpret_cast<const float4*>(sm_wz + 4 * sub);
         wz[0] = w4.x; wz[1] = w4.y; wz[2] = w4.z; wz[3] = w4.w;
     }
-    const bool lane_snap = lane_in && zr >= zs0 && zr < zs0 + lds;
 
 #pragma unroll
     for (int c = 0; c < COLS; ++c) {
-        const int lx = warp * COLS + c;
+        const int base = (c * NWARP + (warp + (unsigned)t.x0 / S::TX) % NWARP) * cpp;
+        if (base >= S::TX) continue;             // warp-uniform
+        const int lx = base + lane / G;
         const int x = t.x0 + lx;
-        const T* col = sm_pc + (lx + H) * S::SZ + 4 * lane + HP;   // row zr of column x
+        const T* col = sm_pc + (lx + H) * S::SZ + 4 * sub + HP;   // row zr of column x
         const bool col_int = (x >= nb) && (x < nb + nx);
         const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
 
@@ -562,8 +585,8 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
         }
 
         T pp[4] = {0, 0, 0, 0}, vd[4];
-        ld4(sm_vd + lx * kTileZ + 4 * lane, vd);
-        if (!first) ld4(sm_pp + lx * kTileZ + 4 * lane, pp);
+        ld4(sm_vd + lx * kTileZ + 4 * sub, vd);
+        if (!first) ld4(sm_pp + lx * kTileZ + 4 * sub, pp);
         T val[4];
         ColumnMath<T, H, EXACT, S::SZ, HP>::run(col, pp, vd, sm_wx[lx], wz, c0, cx, cz, first, val);
         int rkb = 0, rke = 0;
@@ -573,7 +596,7 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
             rke = off[lx + 1];
         }
         column_epilogue<T, H, EXACT>(d, t, x, zr, lane, lane_in, lane_snap, val, vd, fs, Iv, Sv, rkb, rke,
-                                     reinterpret_cast<const RecEntry*>(st + S::REC_OFF), pcur, pnext, ldz);
+                                     reinterpret_cast<const RecEntry*>(st + S::REC_OFF), pcur, pnext, ldz, G);
     }
 }
 
@@ -647,31 +670,47 @@ __device__ __forceinline__ TileInfo decode_tile(const TileRef& tr, long long g) 
 }
 
 // Stages the receivers of columns [x0, x0 + ncols) into re[] with per-column
-// offsets rcs[0..ncols] (warp-cooperative).  Returns false, staging nothing,
-// when the columns hold more than kTileRec receivers.
-__device__ __forceinline__ bool stage_receivers(const ShotDesc& gd, const TileInfo& ti, int x0, int ncols, int nxe,
+// offsets rcs[0..ncols] (warp-cooperative).  Returns false,
+// staging nothing, when the columns hold more than kTileRec receivers.  `sd`
+// is the stage's copy of the descriptor.  Two dependent rounds of global loads
+// (the column offsets, then the receivers' rows, indices and trace samples).
+__device__ __forceinline__ bool stage_receivers(const ShotDesc& sd, const TileInfo& ti, int x0, int ncols, int nxe,
                                                 int* rcs, RecEntry* re) {
     const int lane = threadIdx.x & 31;
-    const int* rec_col = gd.rec_col;
+    const int* rec_col = sd.rec_col;
     if (!rec_col) return false;
+    // column offsets, clamped to nxe (rec_col has nxe + 1 entries)
+    const int xk = x0 + lane < nxe ? x0 + lane : nxe;
     const int xe = x0 + ncols < nxe ? x0 + ncols : nxe;
     const int r_lo = __ldg(rec_col + x0);
     const int nrec = __ldg(rec_col + xe) - r_lo;
+    const int ok = __ldg(rec_col + xk);
     if (nrec > kTileRec) return false;
-    for (int k = lane; k <= ncols; k += 32) {
+    if (lane <= ncols) rcs[lane] = ok - r_lo;
+    for (int k = lane + 32; k <= ncols; k += 32) {
         const int x = x0 + k < nxe ? x0 + k : nxe;
         rcs[k] = __ldg(rec_col + x) - r_lo;
     }
-    const int* pts_ir = gd.pts_ir;
-    const int* rec_zs = gd.rec_zs;
-    const float* traces = gd.traces;
-    const int trace_nt = gd.trace_nt;
-    for (int k = lane; k < nrec; k += 32) {
-        RecEntry e;
-        e.ir = __ldg(pts_ir + r_lo + k);
-        e.z = __ldg(rec_zs + r_lo + k);
-        e.tr = ti.fwd ? 0.f : __ldg(traces + (size_t)e.ir * trace_nt + ti.it);
-        re[k] = e;
+    const int* pts_ir = sd.pts_ir + r_lo;
+    const int* rec_zs = sd.rec_zs + r_lo;
+    constexpr int kPer = kTileRec / 32;
+    int ir[kPer], rz[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int k = lane + 32 * u;
+        ir[u] = k < nrec ? __ldg(pts_ir + k) : 0;
+        rz[u] = k < nrec ? __ldg(rec_zs + k) : 0;
+    }
+    float tr[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int k = lane + 32 * u;
+        tr[u] = (k < nrec && !ti.fwd) ? __ldg(sd.traces + (size_t)ir[u] * sd.trace_nt + ti.it) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int k = lane + 32 * u;
+        if (k < nrec) re[k] = RecEntry{rz[u], ir[u], tr[u]};
     }
     return true;
 }
@@ -679,27 +718,47 @@ __device__ __forceinline__ bool stage_receivers(const ShotDesc& gd, const TileIn
 // Fills one stage with tile `t` (producer warp, all 32 lanes).  Lane 0 decodes
 // what the tile does this step and publishes it as TileInfo; the lanes copy
 // the shot descriptor, the tile's taper weights and (for tiles with receiver
-// cells) the receiver-list offsets into the stage; every lane then arrives on
-// the stage's full barrier (so each lane releases its own writes), lane 0 with
-// the byte count of the TMA boxes it issues.  An active tile always loads
-// (v dt)^2; p^n (with halo) and p^{n-1} are skipped on the first step of a
-// pass, where both are zero.  An inactive tile (its shot is not running at this
-// global step) only publishes TileInfo.
+// cells) the receivers into the stage; every lane then arrives on the stage's
+// full barrier (so each lane releases its own writes), lane 0 with the byte
+// count of the TMA boxes it issues.  An active tile always loads (v dt)^2; p^n
+// (with halo) and p^{n-1} are skipped on the first step of a pass, where both
+// are zero.  An inactive tile (its shot is not running at this global step)
+// only publishes TileInfo.
+//
+// The producer is on the critical path of the pipeline, so its global loads
+// are issued in as few dependent rounds as possible: the descriptor words and
+// both tapers first (before the TMA issue, so their latency overlaps it), the
+// receiver tables after the descriptor has reached shared memory.
 template <typename T, int H, int NWARP, int COLS>
 __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, const CUtensorMap* map_pc,
                                              const CUtensorMap* map_box, const StepParams& p, const TileRef& tr,
                                              long long g) {
     using S = TileShape<T, H, NWARP, COLS>;
+    static_assert(S::TX <= 32, "one producer lane per tile column");
+    static_assert(kTileZ == 4 * 32, "one float4 of the z taper per producer lane");
     const int lane = threadIdx.x & 31;
-    // Decode the step (every lane, identically) and issue the boxes first: they
-    // depend on the TileRef only.
     const TileInfo ti = decode_tile(tr, g);
     if (!ti.active) {
         if (lane == 0) *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
         mbar_arrive(full);
         return;
     }
-    const int x0 = tr.x0, z0 = tr.z0;
+    const int x0 = tr.x0, z0 = tr.z0, nxe = tr.nxe;
+
+    constexpr int kDescWords = (int)(sizeof(ShotDesc) / 4);
+    constexpr int kDescPerLane = (kDescWords + 31) / 32;
+    int dw[kDescPerLane];
+    {
+        const int* src = reinterpret_cast<const int*>(p.descs + tr.slot);
+#pragma unroll
+        for (int k = 0; k < kDescPerLane; ++k)
+            dw[k] = lane + 32 * k < kDescWords ? __ldg(src + lane + 32 * k) : 0;
+    }
+    const int xw = x0 + lane;
+    const float wxv = (lane < S::TX && xw < nxe) ? __ldg(tr.wx + xw) : 0.f;
+    float4 wzv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (z0 + 4 * lane < tr.nze) wzv = __ldg(reinterpret_cast<const float4*>(tr.wz + z0 + 4 * lane));
+
     if (lane == 0) {
         *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
         if (ti.first) {
@@ -711,42 +770,38 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
         }
         tma_load_3d(st + S::VD_OFF, map_box, full, z0, x0, tr.field_base + 2);
     }
-    // The descriptor and the per-tile tables, loaded in parallel by the lanes.
-    const ShotDesc& gd = p.descs[tr.slot];
     {
-        const int* src = reinterpret_cast<const int*>(&gd);
         int* dst = reinterpret_cast<int*>(st + S::DESC_OFF);
-        for (int i = lane; i < (int)(sizeof(ShotDesc) / 4); i += 32) dst[i] = __ldg(src + i);
+#pragma unroll
+        for (int k = 0; k < kDescPerLane; ++k)
+            if (lane + 32 * k < kDescWords) dst[lane + 32 * k] = dw[k];
     }
-    const int nxe = tr.nxe;
-    if (lane < S::TX) {
-        const int x = x0 + lane;
-        reinterpret_cast<float*>(st + S::WX_OFF)[lane] = x < nxe ? __ldg(tr.wx + x) : 0.f;
+    if (lane < S::TX) reinterpret_cast<float*>(st + S::WX_OFF)[lane] = wxv;
+    reinterpret_cast<float4*>(st + S::WZ_OFF)[lane] = wzv;
+    if (!ti.has_pts && !ti.do_image) {
+        mbar_arrive(full);
+        return;
     }
-    {
-        const int z = z0 + 4 * lane;
-        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (z < tr.nze) w = __ldg(reinterpret_cast<const float4*>(tr.wz + z));
-        reinterpret_cast<float4*>(st + S::WZ_OFF)[lane] = w;
-    }
+    __syncwarp();
+    const ShotDesc& sd = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
     if (ti.has_pts) {
         // Stage the tile's receivers (row, index and, backward, this step's
         // trace sample) so consumers never chase the receiver lists in global
         // memory; a tile with more than kTileRec receivers keeps the global path.
-        const bool staged = stage_receivers(gd, ti, x0, S::TX, nxe, reinterpret_cast<int*>(st + S::RCS_OFF),
+        const bool staged = stage_receivers(sd, ti, x0, S::TX, nxe, reinterpret_cast<int*>(st + S::RCS_OFF),
                                             reinterpret_cast<RecEntry*>(st + S::REC_OFF));
         if (!staged)
             for (int k = lane; k <= S::TX; k += 32) {
                 const int x = x0 + k < nxe ? x0 + k : nxe;
-                reinterpret_cast<int*>(st + S::CS_OFF)[k] = __ldg(gd.col_start + x);
+                reinterpret_cast<int*>(st + S::CS_OFF)[k] = __ldg(sd.col_start + x);
             }
         if (lane == 0) reinterpret_cast<TileInfo*>(st + S::INFO_OFF)->rec_staged = staged ? 1 : 0;
     }
     // Stored backward steps: pull the tile's snapshot lines into L2 now, so the
     // consumers' snapshot loads a few tiles later hit L2 instead of HBM.
     if (ti.do_image) {
-        const char* snap = reinterpret_cast<const char*>(gd.snap);
-        const int snap_type = gd.snap_type, zs0 = gd.zs0, lds = gd.lds, nb = gd.nb, nx = gd.nx;
+        const char* snap = reinterpret_cast<const char*>(sd.snap);
+        const int snap_type = sd.snap_type, zs0 = sd.zs0, lds = sd.lds, nb = sd.nb, nx = sd.nx;
         const int es = (snap_type == kSnapF32) ? 4 : (snap_type == kSnapF64 ? 8 : 2);
         const int r0 = z0 > zs0 ? z0 : zs0;
         const int r1 = z0 + kTileZ < zs0 + lds ? z0 + kTileZ : zs0 + lds;
