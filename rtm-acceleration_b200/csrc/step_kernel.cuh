@@ -243,10 +243,14 @@ struct Halo {
 //   [PC_OFF, ..)  TMA box of p^n with the stencil halo      (SZ x SX)
 //   [PP_OFF, ..)  TMA box of p^{n-1}                         (128 x TX)
 //   [VD_OFF, ..)  TMA box of the shot's (v dt)^2             (128 x TX)
-struct TileInfo {
+struct alignas(16) TileInfo {
     int active, fwd, first, it, cur, x0, z0, tz;
     int do_snap, do_image, ksnap, has_pts, rec_staged;
+    int glog;   // log2 of the lanes per column of the band (step kernel)
 };
+static_assert(sizeof(TileInfo) <= 64, "TileInfo fits its block of the stage header");
+
+__host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v / 2); }
 
 constexpr int kTileRec = 128;   // receivers a tile can stage in shared memory
 
@@ -539,15 +543,14 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
     const bool do_image = t.do_image;
 
     // A band with few live rows (the last band of a shot) packs several columns
-    // into one warp: G lanes per column (the fewest float4 lanes that cover the
-    // live rows, a power of two, and at least 32 / TX) and 32 / G columns per
-    // pass.  Passes go round-robin over the warps from a first warp that moves
-    // with the tile's x position, so that the packed bands of successive tiles
-    // land on different warps.  G = 32 is one column per pass.
-    const int live = nze - t.z0 < kTileZ ? nze - t.z0 : kTileZ;
-    int G = 32;
-    while (G > 1 && 4 * (G / 2) >= live && 32 / (G / 2) <= S::TX) G >>= 1;
-    const int cpp = 32 / G;
+    // into one warp: G = 2^t.glog lanes per column (set by the producer) and
+    // 32 / G columns per pass.  Passes go round-robin over the warps from a
+    // first warp that moves with the tile's x position, so that the packed
+    // bands of successive tiles land on different warps.  G = 32 is one column
+    // per pass.
+    const int lg = t.glog;
+    const int G = 1 << lg;
+    const int cpp = 32 >> lg;
     const int sub = lane & (G - 1);              // this thread's float4 slot in the column
     const int zr = t.z0 + 4 * sub;               // first of this thread's 4 rows
     const bool lane_in = zr < nze;
@@ -567,7 +570,7 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
     for (int c = 0; c < COLS; ++c) {
         const int base = (c * NWARP + (warp + (unsigned)t.x0 / S::TX) % NWARP) * cpp;
         if (base >= S::TX) continue;             // warp-uniform
-        const int lx = base + lane / G;
+        const int lx = base + (lane >> lg);
         const int x = t.x0 + lx;
         const T* col = sm_pc + (lx + H) * S::SZ + 4 * sub + HP;   // row zr of column x
         const bool col_int = (x >= nb) && (x < nb + nx);
@@ -736,14 +739,25 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
     using S = TileShape<T, H, NWARP, COLS>;
     static_assert(S::TX <= 32, "one producer lane per tile column");
     static_assert(kTileZ == 4 * 32, "one float4 of the z taper per producer lane");
+    static_assert((S::TX & (S::TX - 1)) == 0, "tile width is a power of two");
     const int lane = threadIdx.x & 31;
-    const TileInfo ti = decode_tile(tr, g);
+    TileInfo ti = decode_tile(tr, g);
     if (!ti.active) {
         if (lane == 0) *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
         mbar_arrive(full);
         return;
     }
     const int x0 = tr.x0, z0 = tr.z0, nxe = tr.nxe;
+    // Lanes per column of the band: the fewest float4 lanes that cover its live
+    // rows (a power of two), and at least 32 / TX so that one pass of a warp
+    // stays inside the tile.
+    {
+        const int live = tr.nze - z0 < kTileZ ? tr.nze - z0 : kTileZ;
+        const int need = (live + 3) >> 2;
+        const int lg = need <= 1 ? 0 : 32 - __clz(need - 1);
+        constexpr int kMinLg = 5 - ilog2(S::TX);
+        ti.glog = lg > kMinLg ? lg : kMinLg;
+    }
 
     constexpr int kDescWords = (int)(sizeof(ShotDesc) / 4);
     constexpr int kDescPerLane = (kDescWords + 31) / 32;
