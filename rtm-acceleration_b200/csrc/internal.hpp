@@ -24,6 +24,7 @@
 namespace rtmb {
 
 constexpr int kMaxHalf = 6;
+constexpr int kCoefSlots = 8;   // cx / cz entries in ShotDesc: kMaxHalf + 1, rounded up to a float4 pair
 constexpr int kTileZ = 128;          // rows per tile: 32 lanes x 4 consecutive rows
 
 enum SnapType : int { kSnapF32 = 0, kSnapBF16 = 1, kSnapF16 = 2, kSnapF64 = 3 };
@@ -66,8 +67,11 @@ struct ShotDesc {
     int acc_mode;
     int field_slot;
     int nrec;
-    // stencil coefficients (float, widened in double kernels)
-    float c0, cx[kMaxHalf + 1], cz[kMaxHalf + 1];
+    // stencil coefficients (float, widened in double kernels); cx and cz start
+    // on 16-byte boundaries so the step kernel reads them as float4 pairs
+    float c0;
+    alignas(16) float cx[kCoefSlots];
+    alignas(16) float cz[kCoefSlots];
     // pointers
     const float* vdt2;       // model table [model_nx][ldz_model]
     int ldz_model;

@@ -280,6 +280,7 @@ struct TileShape {
     static_assert(HDR % 128 == 0, "TMA boxes must start 128-byte aligned");
     static_assert(INFO_OFF + sizeof(TileInfo) <= DESC_OFF, "tile info overflows its block");
     static_assert(DESC_OFF + sizeof(ShotDesc) <= WX_OFF, "descriptor overflows its block");
+    static_assert(STAGE % 128 == 0 && DESC_OFF % 16 == 0, "stages and the descriptor copy are 16-byte aligned");
 };
 
 // Decodes a snapshot value group (4 rows).
@@ -309,9 +310,19 @@ __device__ __forceinline__ void load_snapshot4(const ShotDesc& d, size_t cell, s
 template <typename T, int H, bool EXACT, int SZ, int HP>
 struct ColumnMath {
     static __device__ __forceinline__ void run(const T* col, const T (&pp)[4], const T (&vd)[4], float wxv,
-                                               const float (&wz)[4], T c0, const float* cx, const float* cz,
+                                               const float (&wz)[4], T c0, const float* cxs, const float* czs,
                                                bool first, T (&val)[4]) {
         using A = Arith<T, EXACT>;
+        // coefficients 0..H from the descriptor's 16-byte aligned rows, as float4s
+        constexpr int kChunks = (H + 4) / 4;
+        float cx[4 * kChunks], cz[4 * kChunks];
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            const float4 a = reinterpret_cast<const float4*>(cxs)[c];
+            const float4 b = reinterpret_cast<const float4*>(czs)[c];
+            cx[4 * c] = a.x; cx[4 * c + 1] = a.y; cx[4 * c + 2] = a.z; cx[4 * c + 3] = a.w;
+            cz[4 * c] = b.x; cz[4 * c + 1] = b.y; cz[4 * c + 2] = b.z; cz[4 * c + 3] = b.w;
+        }
         T zz[4 + 2 * HP];
         if (!first) {
 #pragma unroll
@@ -557,7 +568,7 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
     const bool lane_snap = lane_in && zr >= zs0 && zr < zs0 + lds;
 
     const T c0 = (T)d.c0;
-    const float* cx = d.cx;     // read from shared memory where used
+    const float* cx = d.cx;     // read from shared memory (as float4s) where used
     const float* cz = d.cz;
 
     float wz[4];
@@ -871,12 +882,10 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
     const int warp = threadIdx.x >> 5;
 
     if (warp == NWARP) {
-        int i = 0;
+        int s = 0, round = 0;   // stage and how many times the ring has wrapped
         TileRef cur = p.tiles[blockIdx.x];
         TileRef nxt = cur;
-        for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++i) {
-            const int s = i % nst;
-            const int round = i / nst;
+        for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
             if (t + (int)gridDim.x < p.ntiles) nxt = p.tiles[t + gridDim.x];   // in flight while we wait
             if (round > 0 && !mbar_wait_or_abort(empty + s, (round - 1) & 1, abort_flag, p.error_word)) break;
             // Failure-detection test: a tile whose stage is never filled makes the
@@ -887,13 +896,14 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
                 if ((threadIdx.x & 31) == 0) issued[s] = round + 1;
             }
             cur = nxt;
+            if (++s == nst) { s = 0; ++round; }
         }
     } else {
-        int i = 0;
-        for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++i) {
-            const int s = i % nst;
+        int s = 0;
+        uint32_t phase = 0;   // parity of the current round of the ring
+        for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
             const unsigned char* st = stages + (size_t)s * S::STAGE;
-            if (!mbar_wait_or_abort(full + s, (i / nst) & 1, abort_flag, p.error_word)) break;
+            if (!mbar_wait_or_abort(full + s, phase, abort_flag, p.error_word)) break;
             const TileInfo info = *reinterpret_cast<const TileInfo*>(st + S::INFO_OFF);
             if (info.active) {
                 const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
@@ -902,6 +912,7 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
                                                        base + (size_t)(info.cur ^ 1) * p.buf_stride, p.ldz);
             }
             mbar_arrive(empty + s);
+            if (++s == nst) { s = 0; phase ^= 1u; }
         }
     }
     __syncthreads();
