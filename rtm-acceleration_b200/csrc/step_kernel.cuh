@@ -323,29 +323,30 @@ struct ColumnMath {
             cx[4 * c] = a.x; cx[4 * c + 1] = a.y; cx[4 * c + 2] = a.z; cx[4 * c + 3] = a.w;
             cz[4 * c] = b.x; cz[4 * c + 1] = b.y; cz[4 * c + 2] = b.z; cz[4 * c + 3] = b.w;
         }
+        // First step of a pass: p^n = p^{n-1} = 0 and the update below gives +0
+        // in every rounding step (2*0 - 0*w = +0, +0 + vd*(+-0) = +0, +0*w = +0),
+        // so the boxes (not loaded for this step) are not read.
+        if (first) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) val[q] = (T)0;
+            return;
+        }
         T zz[4 + 2 * HP];
-        if (!first) {
 #pragma unroll
-            for (int g = 0; g < (4 + 2 * HP) / 4; ++g) {
-                T tt[4];
-                ld4(col - HP + 4 * g, tt);
+        for (int g = 0; g < (4 + 2 * HP) / 4; ++g) {
+            T tt[4];
+            ld4(col - HP + 4 * g, tt);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) zz[4 * g + q] = tt[q];
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 4 + 2 * HP; ++i) zz[i] = (T)0;
+            for (int q = 0; q < 4; ++q) zz[4 * g + q] = tt[q];
         }
         T lap[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) lap[q] = A::mul(c0, zz[HP + q]);
 #pragma unroll
         for (int k = 1; k <= H; ++k) {
-            T xm[4] = {0, 0, 0, 0}, xp[4] = {0, 0, 0, 0};
-            if (!first) {
-                ld4(col - k * SZ, xm);
-                ld4(col + k * SZ, xp);
-            }
+            T xm[4], xp[4];
+            ld4(col - k * SZ, xm);
+            ld4(col + k * SZ, xp);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const T ax = A::add(xp[q], xm[q]);
@@ -598,9 +599,9 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
             ldg4(reinterpret_cast<const T*>(d.ill) + ic, Sv, 0);
         }
 
-        T pp[4] = {0, 0, 0, 0}, vd[4];
+        T pp[4], vd[4];   // pp is stale on a first step, where ColumnMath does not read it
         ld4(sm_vd + lx * kTileZ + 4 * sub, vd);
-        if (!first) ld4(sm_pp + lx * kTileZ + 4 * sub, pp);
+        ld4(sm_pp + lx * kTileZ + 4 * sub, pp);
         T val[4];
         ColumnMath<T, H, EXACT, S::SZ, HP>::run(col, pp, vd, sm_wx[lx], wz, c0, cx, cz, first, val);
         int rkb = 0, rke = 0;
