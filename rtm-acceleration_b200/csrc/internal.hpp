@@ -120,7 +120,7 @@ struct TileRef {
     const float* wz;     // the model's z taper (ldz)
     int flags;           // ShotFlags of the job
     int nxe, nze;        // extended grid of the shot
-    int pad;
+    int has_src;         // the tile holds the source cell
 };
 static_assert(sizeof(TileRef) == 80, "TileRef layout");
 
@@ -143,6 +143,7 @@ inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int ti
     r.flags = d.flags;
     r.nxe = d.nxe;
     r.nze = d.nze;
+    r.has_src = d.src_x >= r.x0 && d.src_x < r.x0 + tile_x && d.src_z >= r.z0 && d.src_z < r.z0 + kTileZ;
     return r;
 }
 

@@ -247,6 +247,7 @@ struct alignas(16) TileInfo {
     int active, fwd, first, it, cur, x0, z0, tz;
     int do_snap, do_image, ksnap, has_pts, rec_staged;
     int glog;   // log2 of the lanes per column of the band (step kernel)
+    int plain;  // step kernel: no cell of the tile is masked, injects or records
 };
 static_assert(sizeof(TileInfo) <= 64, "TileInfo fits its block of the stage header");
 
@@ -387,51 +388,53 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
     const bool col_live = x < nxe;
     const bool col_int = (x >= nb) && (x < nb + nx);
     const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
-    // the outer H-ring of the grid (and rows/columns past it) stays 0
-    const bool col_ok = (x >= H) && (x < nxe - H);
+    if (!t.plain) {
+        // the outer H-ring of the grid (and rows/columns past it) stays 0
+        const bool col_ok = (x >= H) && (x < nxe - H);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const bool row_ok = (zr + q >= H) && (zr + q < nze - H);
-        val[q] = (col_ok && row_ok) ? val[q] : (T)0;
-    }
+        for (int q = 0; q < 4; ++q) {
+            const bool row_ok = (zr + q >= H) && (zr + q < nze - H);
+            val[q] = (col_ok && row_ok) ? val[q] : (T)0;
+        }
 
-    // Injection at cells whose taper is exactly 1, so adding after the
-    // damping matches the reference's inject-then-damp order bit for bit.
-    if (fwd && x == d.src_x) {
-        const T amp = (T)__ldg(d.wavelet + it);
+        // Injection at cells whose taper is exactly 1, so adding after the
+        // damping matches the reference's inject-then-damp order bit for bit.
+        if (fwd && x == d.src_x) {
+            const T amp = (T)__ldg(d.wavelet + it);
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (zr + q == d.src_z) val[q] = A::add(val[q], A::mul(vd[q], amp));
-    }
-    // Receiver cells of this column: inject (backward) or record (forward
-    // modelling).  Several receivers on one cell add in ascending ir order,
-    // like the reference's sequential loop (backward.cpp:20-27).
-    if (t.has_pts) {
-        if (t.rec_staged) {
-            for (int k = rkb; k < rke; ++k) {
-                const RecEntry e = re[k];
+            for (int q = 0; q < 4; ++q)
+                if (zr + q == d.src_z) val[q] = A::add(val[q], A::mul(vd[q], amp));
+        }
+        // Receiver cells of this column: inject (backward) or record (forward
+        // modelling).  Several receivers on one cell add in ascending ir order,
+        // like the reference's sequential loop (backward.cpp:20-27).
+        if (t.has_pts) {
+            if (t.rec_staged) {
+                for (int k = rkb; k < rke; ++k) {
+                    const RecEntry e = re[k];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (e.z != zr + q) continue;
-                    if (fwd)
-                        stg1(d.rec_out + (size_t)e.ir * d.nt + it, (float)val[q]);
-                    else
-                        val[q] = A::add(val[q], A::mul(vd[q], (T)e.tr));
+                    for (int q = 0; q < 4; ++q) {
+                        if (e.z != zr + q) continue;
+                        if (fwd)
+                            stg1(d.rec_out + (size_t)e.ir * d.nt + it, (float)val[q]);
+                        else
+                            val[q] = A::add(val[q], A::mul(vd[q], (T)e.tr));
+                    }
                 }
-            }
-        } else {
-            for (int j = rkb; j < rke; ++j) {
-                const PointEntry e = d.pts[j];
+            } else {
+                for (int j = rkb; j < rke; ++j) {
+                    const PointEntry e = d.pts[j];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (e.z != zr + q) continue;
-                    for (int r = 0; r < e.ir_count; ++r) {
-                        const int ir = __ldg(d.pts_ir + e.ir_begin + r);
-                        if (fwd) {
-                            stg1(d.rec_out + (size_t)ir * d.nt + it, (float)val[q]);
-                        } else {
-                            const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
-                            val[q] = A::add(val[q], A::mul(vd[q], tr));
+                    for (int q = 0; q < 4; ++q) {
+                        if (e.z != zr + q) continue;
+                        for (int r = 0; r < e.ir_count; ++r) {
+                            const int ir = __ldg(d.pts_ir + e.ir_begin + r);
+                            if (fwd) {
+                                stg1(d.rec_out + (size_t)ir * d.nt + it, (float)val[q]);
+                            } else {
+                                const T tr = (T)__ldg(d.traces + (size_t)ir * d.trace_nt + it);
+                                val[q] = A::add(val[q], A::mul(vd[q], tr));
+                            }
                         }
                     }
                 }
@@ -770,6 +773,11 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
         constexpr int kMinLg = 5 - ilog2(S::TX);
         ti.glog = lg > kMinLg ? lg : kMinLg;
     }
+    // A plain tile needs none of the epilogue's per-cell tests: it lies inside
+    // the ring of H zero cells on every side and holds no source or receiver
+    // work this step.
+    ti.plain = x0 >= H && x0 + S::TX <= nxe - H && z0 >= H && z0 + kTileZ <= tr.nze - H && !ti.has_pts &&
+               !(ti.fwd && tr.has_src);
 
     constexpr int kDescWords = (int)(sizeof(ShotDesc) / 4);
     constexpr int kDescPerLane = (kDescWords + 31) / 32;
