@@ -380,10 +380,21 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
                                                 const RecEntry* __restrict__ re, T* __restrict__ pcur,
                                                 T* __restrict__ pnext, int ldz, int G) {
     using A = Arith<T, EXACT>;
+    const bool first = t.first;
+    const bool do_snap = t.do_snap, do_image = t.do_image;
+    // Plain tile on an unstored step (the common case): every cell of the tile is
+    // live and interior to the zero ring, so the store is all there is.
+    if (t.plain && !do_snap && !do_image) {
+        stg4(pnext + (uint32_t)x * (uint32_t)ldz + zr, val);
+        if (first) {
+            const T z4[4] = {0, 0, 0, 0};
+            stg4(pcur + (uint32_t)x * (uint32_t)ldz + zr, z4);
+        }
+        return;
+    }
     const int nxe = d.nxe, nze = d.nze, nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
     const int it = t.it;
-    const bool fwd = t.fwd, first = t.first;
-    const bool do_snap = t.do_snap, do_image = t.do_image;
+    const bool fwd = t.fwd;
     const int snap_type = d.snap_type;
     const bool col_live = x < nxe;
     const bool col_int = (x >= nb) && (x < nb + nx);
