@@ -2,6 +2,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -807,9 +808,9 @@ int Engine::check_device_error() {
 }
 
 int Engine::admit_from(std::deque<std::pair<Model*, int>>& q, bool modelling, float* rec_base,
-                       const std::vector<size_t>* rec_offsets, int* admitted) {
+                       const std::vector<size_t>* rec_offsets, int* admitted, int limit) {
     *admitted = 0;
-    while (!q.empty()) {
+    while (!q.empty() && (limit < 0 || *admitted < limit)) {
         int free_slot = -1;
         for (int s = 0; s < nslots_; ++s)
             if (!jobs_[(size_t)s].active) { free_slot = s; break; }
@@ -838,19 +839,37 @@ int Engine::admit_from(std::deque<std::pair<Model*, int>>& q, bool modelling, fl
 
 int Engine::run_queue(std::deque<std::pair<Model*, int>>& q, bool modelling, float* rec_base,
                       const std::vector<size_t>* rec_offsets) {
+    // Plain migration with two slots runs shots staggered by one pass: shot s+1
+    // is admitted when shot s starts its backward pass, so s+1's forward pass
+    // overlaps s's backward pass and s+1 images only after s has finished.  Every
+    // image cell still receives its terms in the reference's shot and step order
+    // (bit for bit), and each step launch carries two shots' tiles.
+    const bool staggered = cfg_.mode == RTM_B200_MODE_PLAIN && !modelling && nslots_ > 1;
     while (true) {
         RTMB_TRY(retire_finished());
         int admitted = 0;
-        RTMB_TRY(admit_from(q, modelling, rec_base, rec_offsets, &admitted));
+        if (staggered) {
+            bool in_backward = true;
+            for (const auto& j : jobs_)
+                if (j.active && g_ - j.g0 < j.m->nt) in_backward = false;
+            if (in_backward) RTMB_TRY(admit_from(q, modelling, rec_base, rec_offsets, &admitted, 1));
+        } else {
+            RTMB_TRY(admit_from(q, modelling, rec_base, rec_offsets, &admitted));
+        }
         if (active_jobs() == 0) {
             if (!q.empty()) return fail(RTM_B200_ENOMEM, "a shot does not fit the device memory budget");
             break;
         }
-        int remaining = 0;
-        for (const auto& j : jobs_)
-            if (j.active) remaining = std::max(remaining, (int)(j.total - (g_ - j.g0)));
+        int remaining = 0, next_event = INT_MAX;
+        for (const auto& j : jobs_) {
+            if (!j.active) continue;
+            const int done = (int)(g_ - j.g0);
+            remaining = std::max(remaining, j.total - done);
+            next_event = std::min(next_event, j.total - done);
+            if (!q.empty() && done < j.m->nt) next_event = std::min(next_event, j.m->nt - done);
+        }
         const int c = chunk_for(*jobs_[0].m);
-        RTMB_TRY(run_chunk(std::min(c, remaining)));
+        RTMB_TRY(run_chunk(std::min(c, staggered ? next_event : remaining)));
     }
     return RTM_B200_OK;
 }
@@ -944,6 +963,9 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
     const size_t per_slot = 2 * (size_t)g.nxe * g.ldz * elem() + (size_t)g.nx * g.lds * 16 +
                             (size_t)4 * g.nxe * 3 + (size_t)m.nt * 4 * 2048;
     int want = 1;
+    if (cfg_.mode == RTM_B200_MODE_PLAIN && nshots > 1 &&
+        2 * (per_slot + snap_max) + ((size_t)512 << 20) <= budget)
+        want = 2;   // two shots staggered by one pass (run_queue)
     if (cfg_.mode != RTM_B200_MODE_PLAIN) {
         // 16 shots per launch measured best on the 1150 x 400 workload; more only
         // when asked (the pool and the snapshot arena still bound it).
@@ -954,7 +976,7 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
         want = (int)std::max<size_t>(1, std::min<size_t>((size_t)want, fit));
     }
     RTMB_TRY(ensure_pool(want, g.nxe, g.ldz));
-    size_t arena = cfg_.mode == RTM_B200_MODE_PLAIN ? snap_max
+    size_t arena = cfg_.mode == RTM_B200_MODE_PLAIN ? (size_t)want * snap_max
                                                     : (budget > (size_t)want * per_slot ? budget - (size_t)want * per_slot : 0);
     arena = std::max(arena, snap_max);
     // Keep the current store when it is big enough and not grossly oversized.

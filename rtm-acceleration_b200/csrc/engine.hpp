@@ -149,7 +149,7 @@ private:
     int run_queue(std::deque<std::pair<Model*, int>>& q, bool modelling, float* rec_base,
                   const std::vector<size_t>* rec_offsets);
     int admit_from(std::deque<std::pair<Model*, int>>& q, bool modelling, float* rec_base,
-                   const std::vector<size_t>* rec_offsets, int* admitted);
+                   const std::vector<size_t>* rec_offsets, int* admitted, int limit = -1);
     int active_jobs() const;
     int chunk_for(const Model& m) const;
     int zero_model_images(Model& m);
