@@ -318,20 +318,36 @@ int Engine::ensure_pool(int nslots, int nxe_cap, int ldz_cap) {
     return RTM_B200_OK;
 }
 
+// The largest receiver count and time axis over a model's shots.  Slots are
+// sized for them (and for the full model width), so that shots of other
+// aperture widths reuse the buffers: growing one would cost a device-wide
+// synchronisation (cudaFree / cudaFreeHost) between two chunks of steps.
+static void shot_caps(const Model& m, const ShotData& sh, size_t* nrec, int* nt) {
+    *nrec = (size_t)std::max(sh.nrec, 1);
+    *nt = std::max(sh.nt, m.nt);
+    for (const auto& o : m.shots) {
+        *nrec = std::max(*nrec, (size_t)o.nrec);
+        *nt = std::max(*nt, o.nt);
+    }
+}
+
 int Engine::ensure_slot(int s, const Model& m, const ShotData& sh, const GridDims& gs, bool modelling) {
     Slot& sl = slots_[(size_t)s];
     if (!sl.staged) RTMB_CUDA(cudaEventCreateWithFlags(&sl.staged, cudaEventDisableTiming));
-    const size_t nrec = (size_t)std::max(sh.nrec, 1);
-    RTMB_CUDA(sl.wx.reserve(sizeof(float) * gs.nxe));
-    RTMB_CUDA(sl.col_start.reserve(sizeof(int) * (gs.nxe + 1)));
+    size_t nrec = 0;
+    int nt = 0;
+    shot_caps(m, sh, &nrec, &nt);
+    const int nxe = std::max(gs.nxe, m.g.nxe);
+    RTMB_CUDA(sl.wx.reserve(sizeof(float) * nxe));
+    RTMB_CUDA(sl.col_start.reserve(sizeof(int) * (nxe + 1)));
     RTMB_CUDA(sl.pts.reserve(sizeof(PointEntry) * nrec));
     RTMB_CUDA(sl.ir.reserve(sizeof(int) * nrec));
-    RTMB_CUDA(sl.rec_col.reserve(sizeof(int) * (gs.nxe + 1)));
+    RTMB_CUDA(sl.rec_col.reserve(sizeof(int) * (nxe + 1)));
     RTMB_CUDA(sl.rec_z.reserve(sizeof(int) * nrec));
-    if (!modelling) RTMB_CUDA(sl.traces.reserve(sizeof(float) * nrec * std::max(sh.nt, m.nt)));
+    if (!modelling) RTMB_CUDA(sl.traces.reserve(sizeof(float) * nrec * nt));
     if (modelling) RTMB_CUDA(sl.rec.reserve(sizeof(float) * nrec * m.nt));
     if (cfg_.mode != RTM_B200_MODE_PLAIN && !modelling) {
-        const size_t n = (size_t)gs.nx * gs.lds;
+        const size_t n = std::max((size_t)gs.nx * gs.lds, (size_t)m.g.nx * m.g.lds);
         RTMB_CUDA(sl.acc.reserve(f64_ ? 2 * n * 8 : 4 * n * 4));
     }
     return RTM_B200_OK;
@@ -393,7 +409,19 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     const size_t o_desc = take(sizeof(ShotDesc));
     const size_t o_tr = take(trace_elems * 4);
     RTMB_CUDA(cudaEventSynchronize(sl.staged));   // previous upload from this buffer is done
-    if (cudaSuccess != sl.stage.reserve(off)) {
+    // the same layout for the largest shot of the model (see shot_caps)
+    size_t cap = 0;
+    {
+        size_t nrec_max = 0;
+        int nt_max = 0;
+        shot_caps(*m, sh, &nrec_max, &nt_max);
+        const size_t nxe_max = (size_t)std::max(gs.nxe, m->g.nxe);
+        for (size_t b : {nxe_max * 4, (nxe_max + 1) * 4, nrec_max * sizeof(PointEntry), nrec_max * 4,
+                         (nxe_max + 1) * 4, nrec_max * 4, sizeof(ShotDesc),
+                         trace_elems ? nrec_max * (size_t)nt_max * 4 : (size_t)0})
+            cap += round256(b);
+    }
+    if (cudaSuccess != sl.stage.reserve(std::max(off, cap))) {
         cudaGetLastError();
         return fail(RTM_B200_ENOMEM, "cannot allocate pinned staging memory");
     }
@@ -588,7 +616,10 @@ int Engine::build_tiles() {
     if (all.empty()) return RTM_B200_OK;
     // The device tile list may still be read by queued launches: wait for them.
     RTMB_CUDA(cudaStreamSynchronize(stream_));
-    RTMB_CUDA(tiles_.reserve(all.size() * sizeof(TileRef)));
+    // Room for every slot's largest tile count (16-column tiles over the pool's
+    // width), so that a wider shot mix does not regrow the list mid-run.
+    const size_t most = (size_t)nslots_ * (size_t)((nxe_cap_ + 15) / 16) * (size_t)((ldz_cap_ + kTileZ - 1) / kTileZ);
+    RTMB_CUDA(tiles_.reserve(std::max(all.size(), most) * sizeof(TileRef)));
     RTMB_CUDA(cudaMemcpy(tiles_.get(), all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     for (auto& g : groups_) {
         if (!step_variant_supported(variant(g.half)))
