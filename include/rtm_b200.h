@@ -83,7 +83,7 @@ typedef struct {
     int   snap_precision;   /* RTM_B200_SNAP_*                                 */
     int   arithmetic;       /* RTM_B200_ARITH_*                                */
     int   accumulation;     /* RTM_B200_ACC_* (plain mode always ACC_PLAIN)    */
-    int   max_shots_in_flight; /* batch/serve: 0 = as many as memory allows   */
+    int   max_shots_in_flight; /* batch/serve: 0 = 32 (batch: fewer if short) */
     long long device_mem_budget; /* bytes the engine may hold; 0 = 90% of free */
     int   tile_cols;        /* 0 = autotune; else 16 or 32 columns per tile    */
     int   chunk_steps;      /* time steps per captured CUDA graph, 0 = auto    */
