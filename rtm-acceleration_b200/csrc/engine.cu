@@ -66,8 +66,12 @@ Engine::~Engine() {
         cudaSetDevice(device_);
         cudaStreamSynchronize(stream_);
         if (graph_) cudaGraphExecDestroy(graph_);
-        for (auto& s : slots_)
+        if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+        for (auto& s : slots_) {
             if (s.staged) cudaEventDestroy(s.staged);
+            if (s.free_ev) cudaEventDestroy(s.free_ev);
+            if (s.tr_ready) cudaEventDestroy(s.tr_ready);
+        }
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (tune_ev0_) cudaEventDestroy(tune_ev0_);
@@ -76,6 +80,7 @@ Engine::~Engine() {
             if (e) cudaEventDestroy(e);
         for (auto& f : finishing_)
             if (f && f->ev) cudaEventDestroy(f->ev);
+        if (copy_stream_) cudaStreamDestroy(copy_stream_);
         if (stream_) cudaStreamDestroy(stream_);
     }
 }
@@ -107,6 +112,7 @@ int Engine::init() {
     device_name_ = prop.name;
     if (!tensor_map_encoder()) return fail(RTM_B200_ECUDA, "cuTensorMapEncodeTiled is unavailable");
     RTMB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    RTMB_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     RTMB_CUDA(cudaEventCreate(&ev0_));
     RTMB_CUDA(cudaEventCreate(&ev1_));
     for (auto& e : chunk_ev_) RTMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -334,6 +340,8 @@ static void shot_caps(const Model& m, const ShotData& sh, size_t* nrec, int* nt)
 int Engine::ensure_slot(int s, const Model& m, const ShotData& sh, const GridDims& gs, bool modelling) {
     Slot& sl = slots_[(size_t)s];
     if (!sl.staged) RTMB_CUDA(cudaEventCreateWithFlags(&sl.staged, cudaEventDisableTiming));
+    if (!sl.free_ev) RTMB_CUDA(cudaEventCreateWithFlags(&sl.free_ev, cudaEventDisableTiming));
+    if (!sl.tr_ready) RTMB_CUDA(cudaEventCreateWithFlags(&sl.tr_ready, cudaEventDisableTiming));
     size_t nrec = 0;
     int nt = 0;
     shot_caps(m, sh, &nrec, &nt);
@@ -507,9 +515,22 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     RTMB_CUDA(cudaMemcpyAsync(sl.rec_col.get(), st + o_rc, geo.rec_col.size() * 4, cudaMemcpyHostToDevice, stream_));
     if (!geo.rec_z.empty())
         RTMB_CUDA(cudaMemcpyAsync(sl.rec_z.get(), st + o_rz, geo.rec_z.size() * 4, cudaMemcpyHostToDevice, stream_));
-    if (trace_h2d)
+    job.tr_wait = false;
+    if (trace_h2d && pinned_traces && backward_only == 0) {
+        // A full migration reads its traces from the backward pass on, nt steps
+        // from now: upload them on the copy stream once the work queued so far
+        // (the slot's previous job reads this buffer) is done, so they overlap
+        // the forward pass; run_chunk makes the step stream wait before the
+        // backward pass starts.
+        RTMB_CUDA(cudaEventRecord(sl.free_ev, stream_));
+        RTMB_CUDA(cudaStreamWaitEvent(copy_stream_, sl.free_ev, 0));
+        RTMB_CUDA(cudaMemcpyAsync(sl.traces.get(), sh.traces, trace_h2d * 4, cudaMemcpyHostToDevice, copy_stream_));
+        RTMB_CUDA(cudaEventRecord(sl.tr_ready, copy_stream_));
+        job.tr_wait = true;
+    } else if (trace_h2d) {
         RTMB_CUDA(cudaMemcpyAsync(sl.traces.get(), pinned_traces ? (const void*)sh.traces : (const void*)(st + o_tr),
                                   trace_h2d * 4, cudaMemcpyHostToDevice, stream_));
+    }
     times.h2d_bytes += (double)trace_h2d * 4.0 +
                        (double)(wx.size() * 4 + geo.col_start.size() * 4 + geo.pts.size() * sizeof(PointEntry) +
                                 geo.ir.size() * 4 + geo.rec_col.size() * 4 + geo.rec_z.size() * 4 +
@@ -661,6 +682,7 @@ std::vector<long long> Engine::tune_key() const {
 // After a failed run: drop every job, free its snapshot range and put the
 // device step counter back in step with the host.
 void Engine::abort_jobs() {
+    cudaStreamSynchronize(copy_stream_);
     cudaStreamSynchronize(stream_);
     cudaGetLastError();
     for (auto& j : jobs_) {
@@ -682,6 +704,15 @@ void Engine::abort_jobs() {
 // CUDA events, and the fastest is kept for the mix.  Every candidate computes
 // identical cells, so tuning costs no work.
 int Engine::run_chunk(int steps) {
+    // Traces uploading on the copy stream must land before their job's backward
+    // pass, which may start inside this chunk.
+    for (size_t s = 0; s < jobs_.size(); ++s) {
+        Job& j = jobs_[s];
+        if (j.active && j.tr_wait && g_ + steps > j.g0 + j.m->nt) {
+            RTMB_CUDA(cudaStreamWaitEvent(stream_, slots_[s].tr_ready, 0));
+            j.tr_wait = false;
+        }
+    }
     if (!autotune_ || steps <= 0) return run_steps(steps);
     if (tiles_dirty_ || groups_.empty()) {
         const std::vector<long long> key = tune_key();

@@ -81,12 +81,16 @@ struct Job {
     size_t snap_off = 0, snap_bytes = 0;
     bool owns_snap = false;
     std::vector<std::pair<int, int>> rec_cells;   // (x, z) extended cells holding receivers
+    bool tr_wait = false;              // traces still uploading on the copy stream (run_chunk waits
+                                       // for them before the job's backward pass)
 };
 
 struct Slot {
     DevMem wx, col_start, pts, ir, rec_col, rec_z, traces, rec, acc;
     PinnedMem stage;
     cudaEvent_t staged = nullptr;      // H2D from `stage` finished
+    cudaEvent_t free_ev = nullptr;     // step stream: work queued before a new job's trace upload
+    cudaEvent_t tr_ready = nullptr;    // copy stream: the job's traces have landed
 };
 
 class Engine {
@@ -166,6 +170,7 @@ private:
     std::string error_;
     std::string device_name_;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t copy_stream_ = nullptr;   // trace uploads that overlap the forward pass
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     std::chrono::steady_clock::time_point t0_;
 
