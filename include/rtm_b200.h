@@ -270,20 +270,23 @@ typedef struct {
 /* Forward modelling of one shot (the same kernel and results as
  * rtm_b200_model_shots) that allocates no GPU memory at all.  This entry point
  * has no counterpart in the reference.  It is for callers that cannot call
- * cudaMalloc: code running while a stream is captured into a CUDA graph,
- * plugins whose host owns all device memory through its own pool, and loops
- * that cannot afford the device-wide synchronisation of cudaMalloc/cudaFree.
- * Its scratch (wavefields, tables, receiver lists) lives in a fixed 32 MiB
- * array inside the library's device image, which every GPU that loads the
- * library holds until the process exits; problems whose scratch exceeds it
- * (roughly more than 2.6 million extended cells) are rejected with EINVAL and a
- * message in `err`.  traces_out (nrec*nt, trace-major) may be host memory or
- * device memory of `problem->device`.  The first call on a device looks up the
- * array's device address, so make that first call before any stream capture.
- * Calls share the array; calls that overlap on the GPU would race on it, and
- * this function takes a per-device lock and returns only after its work is
- * done, so calls from one process do not overlap.  Returns a status code; err
- * (may be NULL) receives a message. */
+ * cudaMalloc: plugins whose host application owns every byte of device memory
+ * through its own pool and forbids allocations behind its back, and loops that
+ * cannot afford the device-wide synchronisation that cudaMalloc/cudaFree imply.
+ * The call is synchronous: it copies its tables in, runs, and waits for its own
+ * work before it returns.  Its scratch (wavefields, tables, receiver lists)
+ * lives in a fixed 32 MiB array inside the library's device image, which every
+ * GPU that loads the library holds until the process exits; problems whose
+ * scratch exceeds it (roughly more than 2.6 million extended cells) are
+ * rejected with EINVAL and a message in `err`.  traces_out (nrec*nt,
+ * trace-major) may be host memory or device memory of `problem->device`;
+ * device memory of another GPU is rejected with EINVAL.  The first call on a
+ * device looks up the array's device address, so make that first call before
+ * any stream capture.  Calls share the array and find the previous call's
+ * contents in it; calls that overlapped on the GPU would race on it, so this
+ * function takes a per-device lock and returns only after its work is done,
+ * and calls from one process never overlap.  Returns a status code; err (may be
+ * NULL) receives a message. */
 RTM_B200_API int rtm_b200_model_shot_static(const rtm_b200_static_problem* problem, const rtm_b200_shot* shot,
                                             float* traces_out, char* err, size_t err_len);
 

@@ -1,12 +1,12 @@
 // static_scratch.cu -- forward modelling of one shot without allocating GPU
 // memory (rtm_b200_model_shot_static in include/rtm_b200.h).
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is
-// being captured into a graph (allocation is not allowed during capture), plugins
-// whose host application owns every byte of device memory through its own pool
-// and forbids allocations behind its back, and latency-critical loops where the
-// implicit device synchronisation of cudaMalloc/cudaFree is unacceptable.  For
-// them this file keeps all the scratch the step kernel needs -- the two
+// Some callers cannot call cudaMalloc: plugins whose host application owns
+// every byte of device memory through its own pool and forbids allocations
+// behind its back, and latency-critical loops where the implicit device
+// synchronisation of cudaMalloc/cudaFree is unacceptable.  The call itself is
+// synchronous (plain copies in, the step launches, a wait for its own work).
+// For these callers this file keeps all the scratch the step kernel needs -- the two
 // wavefield levels, the shot's (v dt)^2, the taper and wavelet tables, the
 // receiver lists, the descriptor and the tile list -- in one file-scope device
 // array of fixed size.  The array is part of the library's device image: every
@@ -79,13 +79,18 @@ void set_err(char* err, size_t len, const std::string& m) {
     err[n] = '\0';
 }
 
-bool is_device_memory(const void* p) {
+// Where p lives: 0 host memory (pageable or page-locked), 1 device or managed
+// memory of `device`, -1 device memory of another GPU (the step kernel would
+// write there without peer access).
+int memory_kind(const void* p, int device) {
     cudaPointerAttributes a{};
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return 0;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return 1;
+    if (a.type == cudaMemoryTypeDevice) return a.device == device ? 1 : -1;
+    return 0;
 }
 
 #define SS_CUDA(expr)                                                                  \
@@ -142,7 +147,9 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
         for (int j = geo.col_start[(size_t)x]; j < geo.col_start[(size_t)x + 1]; ++j)
             tflags[(size_t)(x / TX) * g.ntz + geo.pts[(size_t)j].z / kTileZ] = 1;
     const size_t ntiles = (size_t)ntx * g.ntz;
-    const bool out_on_device = is_device_memory(traces_out);
+    const int out_kind = memory_kind(traces_out, pr->device);
+    if (out_kind < 0) throw Fail{RTM_B200_EINVAL, "traces_out is device memory of another GPU than problem->device"};
+    const bool out_on_device = out_kind == 1;
     const size_t nrec = (size_t)std::max(shot->nrec, 0);
 
     // ---- carve the static array ---------------------------------------------

@@ -9,7 +9,7 @@ gathers, ``rtm`` to migrate them) and records:
 * the reference's migrated image and illumination map (``.npy``);
 * the exact parameters of each run (``cases.json``).
 
-Needs the reference tree (default /root/reference, or REF_ROOT); the fixtures
+Needs the reference tree, named by the REF_ROOT environment variable; the fixtures
 it writes are committed, so nothing at test time needs the reference.
 
     python tests/golden/make_golden.py
@@ -113,7 +113,10 @@ def make_case(c, tmp):
 
 
 def main():
-    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    ref_root = os.environ.get("REF_ROOT")
+    if not ref_root:
+        sys.exit("set REF_ROOT to the reference checkout")
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF_ROOT={ref_root}"])
     if not os.path.exists(os.path.join(REF, "rtm")):
         sys.exit("reference binaries are not built (oracle/_ref); is the reference tree present?")
     cases = []

@@ -2,7 +2,7 @@
 outputs, through the C ABI.
 
 Tolerances (the reference's gate is L2rel < 1e-5 and corr > 0.9999,
-src/tools/compare_main.cpp:131-132):
+src/tools/compare_main.cpp:52-53):
   * plain engine, IEEE arithmetic: bit-identical to the reference CPU engine;
   * FMA arithmetic: rel-L2 <= 1e-4 against the FP32 reference (north star);
   * batch engine (compensated FP32 per shot + FP64 stack): rel-L2 <= 1e-5

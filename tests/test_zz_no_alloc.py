@@ -1,14 +1,19 @@
 """The allocation-free modelling entry point, rtm_b200_model_shot_static.
 
-Some callers cannot call cudaMalloc: code that runs while its stream is being
-captured into a CUDA graph, plugins whose host application owns all device
-memory through its own pool, and loops that cannot afford the device-wide
-synchronisation cudaMalloc/cudaFree imply.  For them the library models one
-shot using only a fixed scratch array compiled into its device image.  These
-tests call that entry point through the C ABI twice in a row and check that it
-returns exactly what the ordinary entry point (rtm_b200_model_shots, which
-allocates its buffers) returns, that it leaves free device memory unchanged,
-and that it rejects a problem too large for its scratch with a clear error.
+Some callers cannot call cudaMalloc: plugins whose host application owns all
+device memory through its own pool, and loops that cannot afford the
+device-wide synchronisation cudaMalloc/cudaFree imply.  For them the library
+models one shot using only a fixed scratch array compiled into its device
+image.  These tests call that entry point through the C ABI twice in a row and
+check that it returns exactly what the ordinary entry point
+(rtm_b200_model_shots, which allocates its buffers) returns, that its later
+calls leave free device memory unchanged, that two host threads calling it at
+the same time both get exact results (the per-device lock serialises them on
+the shared array), and that it rejects a problem too large for its scratch
+with a clear error.  The free-memory check starts after the first call on
+purpose: that call loads the library's device module (which holds the array)
+and looks up the array's address, and module loading is not an allocation the
+entry point makes.
 
 This file is named so that pytest collects it last.
 """
@@ -62,6 +67,33 @@ def test_static_modelling_matches_allocating_entry_point_twice():
     rc, msg = _call_static(pr, shot_c, dev.data_ptr())
     assert rc == 0, msg
     assert bits_equal(dev.cpu().numpy(), expected)
+
+
+def test_static_modelling_from_two_threads_at_once():
+    import threading
+    p, v, shots = random_problem(seed=78, order=6, nx=64, nz=40, nb=10, nt=180, si=1)
+    with make_engine("plain", p, v) as e:
+        expected = e.model_shots(shots[:2])
+    pr, vel = _problem(p, v)
+    keep = []
+    shot_cs = [shots_to_c([s], keep) for s in shots[:2]]
+    outs = [np.full(s.nrec * p.nt, np.nan, np.float32) for s in shots[:2]]
+    rcs = [None, None]
+
+    def work(i):
+        for _ in range(3):
+            rcs[i] = _call_static(pr, shot_cs[i], outs[i].ctypes.data)
+            if rcs[i][0] != 0:
+                return
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for i in range(2):
+        assert rcs[i][0] == 0, rcs[i][1]
+        assert bits_equal(outs[i], expected[i])
 
 
 def test_static_modelling_rejects_problems_beyond_its_scratch():
