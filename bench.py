@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument("--max-in-flight", type=int, default=0, help="0 = the engine's default (16)")
     ap.add_argument("--tile-cols", type=int, default=0, help="0 = autotuned")
     ap.add_argument("--snap", default="f32", choices=["f32", "bf16", "f16"])
-    ap.add_argument("--arith", default="ieee", choices=["ieee", "fma"])
+    ap.add_argument("--arith", default="auto", choices=["auto", "ieee", "fma"])
     ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],

@@ -59,6 +59,9 @@ extern "C" {
                                   bit-identical to the reference CPU engine   */
 #define RTM_B200_ARITH_FMA  1  /* FP32 with fused multiply-adds               */
 #define RTM_B200_ARITH_FP64 2  /* FP64 propagation/imaging: the FP64 run      */
+#define RTM_B200_ARITH_AUTO 3  /* IEEE for the plain engine (bit-identical to
+                                  the reference), FMA for batch and serve
+                                  (their sums are compensated, not bitwise)  */
 
 /* ---- accumulation of the per-shot image (batch/serve modes) ------------- */
 #define RTM_B200_ACC_PLAIN        0  /* running FP32 image, reference order    */
@@ -143,7 +146,8 @@ typedef struct {
     double snapshot_bytes;     /* device snapshot footprint per shot            */
 } rtm_b200_request_status;
 
-/* Fill the reference defaults (nb 60, order 8, alpha 0.0053, store 1, f0 12). */
+/* Fill the reference defaults (nb 60, order 8, alpha 0.0053, store 1, f0 12)
+ * and arithmetic RTM_B200_ARITH_AUTO. */
 RTM_B200_API void rtm_b200_config_init(rtm_b200_config* cfg);
 
 /* Create an engine (reference make_engine, include/rtm_factory.hpp:19-20 and

@@ -107,7 +107,7 @@ struct B200Options {
     int mode = RTM_B200_MODE_PLAIN;
     int device = 0;
     int snap_precision = RTM_B200_SNAP_F32;
-    int arithmetic = RTM_B200_ARITH_IEEE;
+    int arithmetic = RTM_B200_ARITH_AUTO;
     int accumulation = RTM_B200_ACC_COMPENSATED;
     int max_shots_in_flight = 0;
     int tile_cols = 0;

@@ -55,7 +55,7 @@ void rtm_b200_config_init(rtm_b200_config* c) {
     c->f0 = 12.0f;
     c->verbose = 0;
     c->snap_precision = RTM_B200_SNAP_F32;
-    c->arithmetic = RTM_B200_ARITH_IEEE;
+    c->arithmetic = RTM_B200_ARITH_AUTO;
     c->accumulation = RTM_B200_ACC_COMPENSATED;
 }
 
@@ -166,8 +166,8 @@ int rtm_b200_autotune_report(const rtm_b200_engine* h, char* buf, size_t len) {
             js += t;
         }
         auto choice = [](const rtmb::Engine::TuneChoice& c) {
-            return std::string("{\"kernel\": \"") + (c.kind == 1 ? "march" : "ring") + "\", \"cols\": " +
-                   std::to_string(c.cols) + ", \"stages\": " + std::to_string(c.stages) + ", \"march_m\": " +
+            return std::string("{\"kernel\": \"") + (c.kind == 1 ? "march" : "ring") + "\", \"warps\": " +
+                   std::to_string(c.warps) + ", \"tile_x\": " + std::to_string(c.tile_x) + ", \"stages\": " + std::to_string(c.stages) + ", \"march_m\": " +
                    std::to_string(c.march_m) + "}";
         };
         js += "], \"candidates\": [";

@@ -57,7 +57,15 @@ bool is_pinned_ptr(const void* p) {
 }  // namespace
 
 Engine::Engine(const rtm_b200_config& cfg) : cfg_(cfg) {
-    f64_ = cfg.arithmetic == RTM_B200_ARITH_FP64;
+    // AUTO: the plain engine keeps the reference's unfused IEEE arithmetic (bit
+    // for bit); batch and serve, whose per-shot sums are compensated and whose
+    // gate is a tolerance against FP64, use fused multiply-adds.
+    // Modelling (the synthetic-data generator) always runs IEEE under AUTO, so
+    // that its shot files are the reference's byte for byte.
+    auto_arith_ = cfg_.arithmetic == RTM_B200_ARITH_AUTO;
+    if (auto_arith_)
+        cfg_.arithmetic = cfg_.mode == RTM_B200_MODE_PLAIN ? RTM_B200_ARITH_IEEE : RTM_B200_ARITH_FMA;
+    f64_ = cfg_.arithmetic == RTM_B200_ARITH_FP64;
     t0_ = std::chrono::steady_clock::now();
 }
 
@@ -121,7 +129,8 @@ int Engine::init() {
     RTMB_CUDA(cudaMemsetAsync(counter_.get(), 0, sizeof(long long), stream_));
     RTMB_CUDA(cudaMemsetAsync(errword_.get(), 0, sizeof(int), stream_));
     RTMB_CUDA(cudaStreamSynchronize(stream_));
-    cols_ = cfg_.tile_cols == 32 ? 4 : 2;
+    tile_x_ = cfg_.tile_cols == 32 ? 32 : 16;
+    warps_ = tile_x_ == 32 ? 8 : 4;
     autotune_ = cfg_.tile_cols == 0;
     // Failure-detection test hook: the first step launch leaves this tile's
     // stage empty, so the kernel's bounded wait must give up and report.
@@ -270,8 +279,9 @@ StepVariant Engine::variant(int half) const {
     StepVariant v;
     v.f64 = f64_;
     v.half = half;
-    v.cols = cols_;
-    v.exact = cfg_.arithmetic == RTM_B200_ARITH_IEEE;
+    v.tile_x = tile_x_;
+    v.warps = f64_ ? 8 : warps_;
+    v.exact = exact();
     v.kind = f64_ ? kStepRing : kind_;
     v.march_m = march_m_;
     v.nstage = step_default_stages(v);
@@ -621,7 +631,9 @@ int Engine::build_tiles() {
         sig.push_back(j.total);
         sig.push_back(d.flags);
     }
-    sig.push_back(cols_);
+    sig.push_back(tile_x_);
+    sig.push_back(warps_);
+    sig.push_back(exact() ? 1 : 0);
     sig.push_back(stage_override_);
     sig.push_back(kind_);
     sig.push_back(march_m_);
@@ -644,9 +656,9 @@ int Engine::build_tiles() {
     RTMB_CUDA(cudaMemcpy(tiles_.get(), all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     for (auto& g : groups_) {
         if (!step_variant_supported(variant(g.half)))
-            return fail(RTM_B200_EUNSUPPORTED, "tile width " + std::to_string(8 * cols_) + " does not fit shared memory "
+            return fail(RTM_B200_EUNSUPPORTED, "tile width " + std::to_string(tile_x_) + " does not fit shared memory "
                         "for this stencil order and precision (use tile_cols 0 or 16)");
-        const int mk = g.half * 16 + cols_;
+        const int mk = g.half * 64 + tile_x_;
         if (variant(g.half).kind == kStepRing && !maps_.count(mk)) {
             MapPair mp;
             RTMB_TRY(encode_map(g.half, true, &mp.pc));
@@ -676,6 +688,7 @@ std::vector<long long> Engine::tune_key() const {
     while (b < n) b *= 2;
     k.push_back(b);
     k.push_back(f64_ ? 1 : 0);
+    k.push_back(exact() ? 1 : 0);
     return k;
 }
 
@@ -718,18 +731,26 @@ int Engine::run_chunk(int steps) {
         const std::vector<long long> key = tune_key();
         auto hit = tuned_.find(key);
         auto apply = [&](const TuneChoice& c) {
-            if (kind_ != c.kind || cols_ != c.cols || stage_override_ != c.stages || march_m_ != c.march_m)
+            if (kind_ != c.kind || warps_ != c.warps || tile_x_ != c.tile_x || stage_override_ != c.stages ||
+                march_m_ != c.march_m)
                 tiles_dirty_ = true;
             kind_ = c.kind;
-            cols_ = c.cols;
+            warps_ = c.warps;
+            tile_x_ = c.tile_x;
             stage_override_ = c.stages;
             march_m_ = c.march_m;
         };
         if (hit != tuned_.end()) {
             apply(hit->second);
         } else {
-            std::vector<TuneChoice> cands = {{kStepRing, 2, 0, 3}, {kStepRing, 2, 2, 3}, {kStepRing, 4, 0, 3},
-                                             {kStepMarch, 2, 0, 2}, {kStepMarch, 2, 0, 3}, {kStepMarch, 2, 0, 5}};
+            // Ring shapes (consumer warps x tile width, default stages) and the
+            // register-march strip lengths.  The march kernel's FMA arithmetic
+            // is not the ring kernel's, so with FMA it is not a candidate: every
+            // candidate of a mix must compute the same cells.
+            std::vector<TuneChoice> cands = {{kStepRing, 4, 16, 0, 3}, {kStepRing, 8, 16, 0, 3},
+                                             {kStepRing, 8, 32, 0, 3}};
+            if (exact())
+                for (int m : {2, 3, 5}) cands.push_back({kStepMarch, 8, 16, 0, m});
             if (pin_kind_ >= 0) {
                 std::vector<TuneChoice> keep;
                 for (const auto& c : cands)
@@ -812,7 +833,7 @@ int Engine::run_steps(int steps) {
                 }
                 p.march_m = v.march_m;
                 static const MapPair kNoMaps{};
-                const MapPair& mp = v.kind == kStepRing ? maps_[g.half * 16 + cols_] : kNoMaps;
+                const MapPair& mp = v.kind == kStepRing ? maps_[g.half * 64 + tile_x_] : kNoMaps;
                 RTMB_CUDA(launch_step(v, mp.pc, mp.box, p, stream_));
             }
         RTMB_CUDA(launch_advance_counter(counter_.get<long long>(), steps, stream_));
@@ -1088,6 +1109,11 @@ int Engine::model_shots(const rtm_b200_shot* shots, int nshots, float* out) {
     Model& m = *model_;
     RTMB_TRY(copy_shots(m, shots, nshots, false));
     keep_snap_ = false;
+    struct ModellingScope {   // IEEE arithmetic for the duration of the call (AUTO)
+        Engine* e;
+        explicit ModellingScope(Engine* en) : e(en) { e->modelling_now_ = true; e->tiles_dirty_ = true; }
+        ~ModellingScope() { e->modelling_now_ = false; e->tiles_dirty_ = true; }
+    } scope(this);
     std::vector<size_t> offs((size_t)nshots);
     size_t acc = 0;
     for (int i = 0; i < nshots; ++i) {

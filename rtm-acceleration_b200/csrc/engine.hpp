@@ -165,6 +165,11 @@ private:
 
     rtm_b200_config cfg_{};
     bool f64_ = false;
+    bool auto_arith_ = false;                // arithmetic AUTO: modelling runs IEEE
+    bool modelling_now_ = false;             // inside model_shots
+    bool exact() const {
+        return cfg_.arithmetic == RTM_B200_ARITH_IEEE || (auto_arith_ && modelling_now_);
+    }
     bool inited_ = false;
     int device_ = 0;
     std::string error_;
@@ -180,7 +185,7 @@ private:
     DevMem pool_;
     int nslots_ = 0, nxe_cap_ = 0, ldz_cap_ = 0;
     struct MapPair { CUtensorMap pc, box; };
-    std::map<int, MapPair> maps_;            // by (half, cols): p^n box with halo; 128 x TX box
+    std::map<int, MapPair> maps_;            // by (half, tile width): p^n box with halo; 128 x TX box
     std::vector<Slot> slots_;
     std::vector<Job> jobs_;
     DevMem descs_;                           // ShotDesc[nslots]
@@ -204,7 +209,8 @@ private:
     std::vector<long long> graph_sig_;
     int graph_steps_ = 0;
     int launches_ = 0;
-    int cols_ = 4;                           // ring kernel: columns per consumer warp
+    int tile_x_ = 16;                        // ring kernel: tile width (16 or 32 columns)
+    int warps_ = 4;                          // ring kernel: consumer warps per CTA
     int stage_override_ = 0;                 // ring kernel: pipeline stages (0 = default)
     int stall_tile_ = -1;                    // failure-detection test hook (RTM_B200_STALL_TILE)
     // Autotuner: the fastest step kernel and parameters measured on real steps,
@@ -214,7 +220,7 @@ private:
     int march_m_ = 3;                        // march strip length, units of 2H+1 columns
     int pin_kind_ = -1;                      // step kernel pinned by RTM_B200_STEP_KERNEL (-1: tuned)
 public:
-    struct TuneChoice { int kind, cols, stages, march_m; };
+    struct TuneChoice { int kind, warps, tile_x, stages, march_m; };
 private:
     std::map<std::vector<long long>, TuneChoice> tuned_;
     std::vector<long long> tune_key() const;

@@ -16,29 +16,29 @@ namespace {
 
 // Largest dynamic shared-memory request of a variant (kMaxStages stages, capped
 // at the 227 KB a CTA may use); set once, so any stage count up to it launches.
-template <typename T, int H, int COLS>
+template <typename T, int H, int NCW, int TX>
 int max_smem_impl() {
-    using S = TileShape<T, H, kStepWarps, COLS>;
+    using S = TileShape<T, H, NCW, TX>;
     int n = kMaxStages;
     while (n > 2 && kCtrlBytes + n * S::STAGE > 227 * 1024) --n;
     return kCtrlBytes + n * S::STAGE;
 }
 
-template <typename T, int H, bool EX, int COLS>
+template <typename T, int H, bool EX, int NCW, int TX>
 cudaError_t attr_impl() {
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(step_kernel<T, H, EX, kStepWarps, COLS>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_impl<T, H, COLS>());
+        attr_err = cudaFuncSetAttribute(step_kernel<T, H, EX, NCW, TX>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_impl<T, H, NCW, TX>());
     });
     return attr_err;
 }
 
 // Resident CTAs per device for a stage count (the persistent grid size).
-template <typename T, int H, bool EX, int COLS>
+template <typename T, int H, bool EX, int NCW, int TX>
 int max_grid_impl(int nstage) {
-    using S = TileShape<T, H, kStepWarps, COLS>;
+    using S = TileShape<T, H, NCW, TX>;
     static std::mutex mu;
     static int cache[kMaxStages + 1] = {};
     std::lock_guard<std::mutex> lk(mu);
@@ -48,9 +48,10 @@ int max_grid_impl(int nstage) {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const int smem = kCtrlBytes + nstage * S::STAGE;
-        if (smem <= max_smem_impl<T, H, COLS>() && attr_impl<T, H, EX, COLS>() == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_kernel<T, H, EX, kStepWarps, COLS>,
-                                                          kStepThreads, smem) == cudaSuccess && per > 0)
+        if (smem <= max_smem_impl<T, H, NCW, TX>() && attr_impl<T, H, EX, NCW, TX>() == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_kernel<T, H, EX, NCW, TX>,
+                                                          (NCW + 1) * 32, smem) == cudaSuccess &&
+            per > 0)
             cache[nstage] = sms * per;
         else
             cache[nstage] = -1;
@@ -58,16 +59,21 @@ int max_grid_impl(int nstage) {
     return cache[nstage] > 0 ? cache[nstage] : 0;
 }
 
-template <typename T, int H, bool EX, int COLS>
+template <typename T, int H, int NCW, int TX>
+int stage_bytes_impl() {
+    return TileShape<T, H, NCW, TX>::STAGE;
+}
+
+template <typename T, int H, bool EX, int NCW, int TX>
 cudaError_t launch_impl(const CUtensorMap& mpc, const CUtensorMap& mpp, const StepParams& p, cudaStream_t s) {
-    using S = TileShape<T, H, kStepWarps, COLS>;
-    const cudaError_t e = attr_impl<T, H, EX, COLS>();
+    using S = TileShape<T, H, NCW, TX>;
+    const cudaError_t e = attr_impl<T, H, EX, NCW, TX>();
     if (e != cudaSuccess) return e;
-    const int cap = max_grid_impl<T, H, EX, COLS>(p.nstage);
+    const int cap = max_grid_impl<T, H, EX, NCW, TX>(p.nstage);
     if (cap <= 0) return cudaErrorInvalidConfiguration;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)(p.ntiles < cap ? p.ntiles : cap));
-    cfg.blockDim = dim3(kStepThreads);
+    cfg.blockDim = dim3((NCW + 1) * 32);
     cfg.dynamicSmemBytes = (size_t)(kCtrlBytes + p.nstage * S::STAGE);
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -75,47 +81,57 @@ cudaError_t launch_impl(const CUtensorMap& mpc, const CUtensorMap& mpp, const St
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = p.pdl ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, step_kernel<T, H, EX, kStepWarps, COLS>, mpc, mpp, p);
+    return cudaLaunchKernelEx(&cfg, step_kernel<T, H, EX, NCW, TX>, mpc, mpp, p);
 }
 
-template <typename T, bool EX, int COLS>
-cudaError_t by_half(int half, const CUtensorMap& a, const CUtensorMap& b, const StepParams& p, cudaStream_t s) {
-    switch (half) {
-        case 1: return launch_impl<T, 1, EX, COLS>(a, b, p, s);
-        case 2: return launch_impl<T, 2, EX, COLS>(a, b, p, s);
-        case 3: return launch_impl<T, 3, EX, COLS>(a, b, p, s);
-        case 4: return launch_impl<T, 4, EX, COLS>(a, b, p, s);
-        case 5: return launch_impl<T, 5, EX, COLS>(a, b, p, s);
-        case 6: return launch_impl<T, 6, EX, COLS>(a, b, p, s);
-        default: return cudaErrorInvalidValue;
+// Calls F::template run<T, H, EX, NCW, TX>(args...) for the variant's run-time
+// choices (element type, half order, arithmetic, consumer warps, tile width).
+template <typename F, typename R, typename... A>
+R dispatch(const StepVariant& v, R bad, A&&... a) {
+#define RTMB_HALVES(T, EX, NCW, TX)                                            \
+    switch (v.half) {                                                          \
+        case 1: return F::template run<T, 1, EX, NCW, TX>(a...);               \
+        case 2: return F::template run<T, 2, EX, NCW, TX>(a...);               \
+        case 3: return F::template run<T, 3, EX, NCW, TX>(a...);               \
+        case 4: return F::template run<T, 4, EX, NCW, TX>(a...);               \
+        case 5: return F::template run<T, 5, EX, NCW, TX>(a...);               \
+        case 6: return F::template run<T, 6, EX, NCW, TX>(a...);               \
+        default: return bad;                                                   \
     }
+#define RTMB_SHAPES(T, EX)                                                     \
+    if (v.warps == 4 && v.tile_x == 16) { RTMB_HALVES(T, EX, 4, 16) }          \
+    if (v.warps == 8 && v.tile_x == 16) { RTMB_HALVES(T, EX, 8, 16) }          \
+    if (v.warps == 8 && v.tile_x == 32) { RTMB_HALVES(T, EX, 8, 32) }          \
+    return bad;
+    if (!step_shape_supported(v.f64, v.warps, v.tile_x)) return bad;
+    if (v.f64) {
+        if (v.tile_x == 32) { RTMB_HALVES(double, false, 8, 32) }
+        RTMB_HALVES(double, false, 8, 16)
+    }
+    if (v.exact) { RTMB_SHAPES(float, true) }
+    RTMB_SHAPES(float, false)
+#undef RTMB_SHAPES
+#undef RTMB_HALVES
 }
 
-template <typename T, bool EX, int COLS>
-int grid_by_half(int half, int nstage) {
-    switch (half) {
-        case 1: return max_grid_impl<T, 1, EX, COLS>(nstage);
-        case 2: return max_grid_impl<T, 2, EX, COLS>(nstage);
-        case 3: return max_grid_impl<T, 3, EX, COLS>(nstage);
-        case 4: return max_grid_impl<T, 4, EX, COLS>(nstage);
-        case 5: return max_grid_impl<T, 5, EX, COLS>(nstage);
-        case 6: return max_grid_impl<T, 6, EX, COLS>(nstage);
-        default: return 0;
+struct LaunchF {
+    template <typename T, int H, bool EX, int NCW, int TX>
+    static cudaError_t run(const CUtensorMap& a, const CUtensorMap& b, const StepParams& p, cudaStream_t s) {
+        return launch_impl<T, H, EX, NCW, TX>(a, b, p, s);
     }
-}
-
-template <typename T, bool EX, int COLS>
-cudaError_t attr_by_half(int half) {
-    switch (half) {
-        case 1: return attr_impl<T, 1, EX, COLS>();
-        case 2: return attr_impl<T, 2, EX, COLS>();
-        case 3: return attr_impl<T, 3, EX, COLS>();
-        case 4: return attr_impl<T, 4, EX, COLS>();
-        case 5: return attr_impl<T, 5, EX, COLS>();
-        case 6: return attr_impl<T, 6, EX, COLS>();
-        default: return cudaErrorInvalidValue;
-    }
-}
+};
+struct GridF {
+    template <typename T, int H, bool EX, int NCW, int TX>
+    static int run(int nstage) { return max_grid_impl<T, H, EX, NCW, TX>(nstage); }
+};
+struct AttrF {
+    template <typename T, int H, bool EX, int NCW, int TX>
+    static cudaError_t run() { return attr_impl<T, H, EX, NCW, TX>(); }
+};
+struct StageF {
+    template <typename T, int H, bool EX, int NCW, int TX>
+    static int run() { return stage_bytes_impl<T, H, NCW, TX>(); }
+};
 
 }  // namespace
 
@@ -170,43 +186,32 @@ cudaError_t prepare_step(const StepVariant& v) {
     if (!step_variant_supported(v)) return cudaErrorInvalidValue;
     if (v.kind == kStepMarch) return cudaSuccess;
     if (step_max_grid(v) <= 0) return cudaErrorInvalidValue;
-    if (v.f64) return v.cols == 4 ? attr_by_half<double, false, 4>(v.half) : attr_by_half<double, false, 2>(v.half);
-    if (v.exact) return v.cols == 4 ? attr_by_half<float, true, 4>(v.half) : attr_by_half<float, true, 2>(v.half);
-    return v.cols == 4 ? attr_by_half<float, false, 4>(v.half) : attr_by_half<float, false, 2>(v.half);
+    return dispatch<AttrF>(v, cudaErrorInvalidValue);
 }
 
 bool step_variant_supported(const StepVariant& v) {
     if (v.half < 1 || v.half > kMaxHalf) return false;
     if (v.kind == kStepMarch) return !v.f64 && v.march_m >= 1 && v.march_m <= 9;
     if (v.kind != kStepRing) return false;
-    if (v.cols != 2 && v.cols != 4) return false;
+    if (!step_shape_supported(v.f64, v.warps, v.tile_x)) return false;
     if (v.nstage < 2 || v.nstage > kMaxStages) return false;
     return step_smem_bytes(v) <= 227 * 1024;
 }
 
-int step_stage_bytes(const StepVariant& v) {
-    const int elem = v.f64 ? 8 : 4;
-    const int pc = step_box_z(v) * step_box_x(v) * elem;
-    const int box = kTileZ * step_tile_x(v) * elem;
-    return 1408 + ((pc + 127) & ~127) + 2 * ((box + 127) & ~127);
-}
+int step_stage_bytes(const StepVariant& v) { return dispatch<StageF>(v, 1 << 30); }
 
 int step_smem_bytes(const StepVariant& v) { return kCtrlBytes + v.nstage * step_stage_bytes(v); }
 
 int step_default_stages(const StepVariant& v) {
-    // Deepest ring that still lets two FP32 CTAs share an SM (228 KB, 1 KB
-    // reserved per CTA); otherwise (FP64, or tiles too large for two CTAs) the
-    // deepest ring one CTA can hold.
+    // Deepest ring that keeps the variant's CTAs per SM inside the SM's 228 KB
+    // (1 KB reserved per CTA) and a CTA's 227 KB.
     StepVariant t = v;
     const int per_sm = 228 * 1024;
-    if (!v.f64)
-        for (int n = kMaxStages; n >= 2; --n) {
-            t.nstage = n;
-            if (2 * (step_smem_bytes(t) + 1024) <= per_sm) return n;
-        }
+    const int ctas = step_ctas_per_sm(v);
     for (int n = kMaxStages; n >= 2; --n) {
         t.nstage = n;
-        if (step_smem_bytes(t) <= 227 * 1024) return n;
+        const int b = step_smem_bytes(t);
+        if (b <= 227 * 1024 && ctas * (b + 1024) <= per_sm) return n;
     }
     return 2;
 }
@@ -214,14 +219,7 @@ int step_default_stages(const StepVariant& v) {
 int step_max_grid(const StepVariant& v) {
     if (!step_variant_supported(v)) return 0;
     if (v.kind == kStepMarch) return 1;
-    if (v.f64)
-        return v.cols == 4 ? grid_by_half<double, false, 4>(v.half, v.nstage)
-                           : grid_by_half<double, false, 2>(v.half, v.nstage);
-    if (v.exact)
-        return v.cols == 4 ? grid_by_half<float, true, 4>(v.half, v.nstage)
-                           : grid_by_half<float, true, 2>(v.half, v.nstage);
-    return v.cols == 4 ? grid_by_half<float, false, 4>(v.half, v.nstage)
-                       : grid_by_half<float, false, 2>(v.half, v.nstage);
+    return dispatch<GridF>(v, 0, v.nstage);
 }
 
 cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUtensorMap& mpp, const StepParams& pin,
@@ -231,16 +229,7 @@ cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUte
     p.nstage = v.nstage;
     p.march_m = v.march_m;
     if (v.kind == kStepMarch) return v.exact ? march_by_half<true>(v.half, p, s) : march_by_half<false>(v.half, p, s);
-    if (v.f64) {
-        if (v.cols == 4) return by_half<double, false, 4>(v.half, mpc, mpp, p, s);
-        return by_half<double, false, 2>(v.half, mpc, mpp, p, s);
-    }
-    if (v.exact) {
-        if (v.cols == 4) return by_half<float, true, 4>(v.half, mpc, mpp, p, s);
-        return by_half<float, true, 2>(v.half, mpc, mpp, p, s);
-    }
-    if (v.cols == 4) return by_half<float, false, 4>(v.half, mpc, mpp, p, s);
-    return by_half<float, false, 2>(v.half, mpc, mpp, p, s);
+    return dispatch<LaunchF>(v, cudaErrorInvalidValue, mpc, mpp, p, s);
 }
 
 cudaError_t launch_advance_counter(long long* counter, int by, cudaStream_t s) {

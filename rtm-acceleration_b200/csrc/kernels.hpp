@@ -14,7 +14,8 @@ struct StepVariant {
     bool f64 = false;   // double fields (the FP64 run)
     int half = 4;       // order / 2
     bool exact = true;  // IEEE unfused float arithmetic (bit-identical path)
-    int cols = 4;       // columns per consumer warp; tile is 128 rows x (8*cols) columns
+    int tile_x = 16;    // ring kernel: tile of 128 rows x tile_x (16 or 32) columns
+    int warps = 8;      // ring kernel: consumer warps per CTA (see step_shape_supported)
     int nstage = 3;     // shared-memory pipeline stages, 2..kMaxStages
     int kind = 0;       // 0: TMA ring kernel (step_kernel); 1: register march (march_kernel, FP32)
     int march_m = 3;    // march: strip length in units of 2*half+1 columns (1..9)
@@ -23,11 +24,28 @@ struct StepVariant {
 constexpr int kStepRing = 0;
 constexpr int kStepMarch = 1;
 
-constexpr int kStepWarps = 8;                        // consumer warps
-constexpr int kStepThreads = (kStepWarps + 1) * 32;  // + the producer warp
+// Ring-kernel shapes (consumer warps x tile width) and the CTAs per SM each is
+// built for.  An SM's registers are split over its four sub-partitions and
+// warps are dealt to them round-robin, so the per-thread register budget
+// follows the most loaded sub-partition:
+//   FP32  4 warps x 16 columns, 3 CTAs/SM (15 warps: 128 registers), 2 column
+//         pairs per warp per tile;
+//   FP32  8 warps x 16 columns, 2 CTAs/SM (18 warps:  96 registers), 1 pair;
+//   FP32  8 warps x 32 columns, 1 CTA/SM  ( 9 warps: 168 registers), 2 pairs;
+//   FP64  8 warps x 16 or 32 columns, 1 CTA/SM.
+inline bool step_shape_supported(bool f64, int warps, int tile_x) {
+    if (f64) return warps == 8 && (tile_x == 16 || tile_x == 32);
+    return (warps == 4 && tile_x == 16) || (warps == 8 && (tile_x == 16 || tile_x == 32));
+}
+template <typename T, int NCW, int TX>
+constexpr int step_ctas_per_sm() { return sizeof(T) == 8 ? 1 : (NCW == 4 ? 3 : (TX == 16 ? 2 : 1)); }
+inline int step_ctas_per_sm(const StepVariant& v) {
+    return v.f64 ? 1 : (v.warps == 4 ? 3 : (v.tile_x == 16 ? 2 : 1));
+}
+inline int step_threads(const StepVariant& v) { return (v.warps + 1) * 32; }
 
 inline int step_tile_x(const StepVariant& v) {
-    return v.kind == kStepMarch ? (2 * v.half + 1) * v.march_m : kStepWarps * v.cols;
+    return v.kind == kStepMarch ? (2 * v.half + 1) * v.march_m : v.tile_x;
 }
 inline int step_halo_rows(const StepVariant& v) { return (v.half + 3) & ~3; }
 inline int step_box_z(const StepVariant& v) { return kTileZ + 2 * step_halo_rows(v); }
@@ -35,7 +53,8 @@ inline int step_box_x(const StepVariant& v) { return step_tile_x(v) + 2 * v.half
 int step_stage_bytes(const StepVariant& v);
 int step_smem_bytes(const StepVariant& v);
 bool step_variant_supported(const StepVariant& v);
-// Deepest pipeline that keeps two CTAs per SM (FP32) / fits one CTA (FP64).
+// Deepest pipeline that keeps the variant's CTAs per SM (step_ctas_per_sm)
+// inside the SM's shared memory.
 int step_default_stages(const StepVariant& v);
 
 // Sets the kernel's shared-memory attribute (call before any stream capture).

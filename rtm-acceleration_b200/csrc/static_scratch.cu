@@ -135,7 +135,8 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     const GridDims g = make_grid(pr->nx, pr->nz, pr->nb, half);
     StepVariant v;
     v.half = half;
-    v.cols = 2;
+    v.tile_x = 16;
+    v.warps = 4;
     v.exact = true;
     v.nstage = step_default_stages(v);
     const int TX = step_tile_x(v);

@@ -11,7 +11,8 @@
 //      lane issues 3D TMA box loads of p^n (tile + stencil halo), p^{n-1} and the
 //      shot's (v dt)^2 against the stage's "full" mbarrier;
 //   2. eight consumer warps wait on "full", each thread owns 4 consecutive depth
-//      cells (a float4) of COLS columns and evaluates the order-2H Laplacian
+//      cells (a float4) of its share of the tile's columns and evaluates the
+//      order-2H Laplacian
 //      from shared memory, then releases the stage on its "empty" mbarrier;
 //   3. p^{n+1} = w (2 p^n - w p^{n-1} + vdt2 lap) + injection, written in place
 //      over p^{n-1} (only the owning thread touches that cell, so two time
@@ -248,6 +249,7 @@ struct alignas(16) TileInfo {
     int do_snap, do_image, ksnap, has_pts, rec_staged;
     int glog;   // log2 of the lanes per column of the band (step kernel)
     int plain;  // step kernel: no cell of the tile is masked, injects or records
+    int unitw;  // step kernel: every live cell of the tile has sponge weight exactly 1
 };
 static_assert(sizeof(TileInfo) <= 64, "TileInfo fits its block of the stage header");
 
@@ -255,10 +257,11 @@ __host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v
 
 constexpr int kTileRec = 128;   // receivers a tile can stage in shared memory
 
-template <typename T, int H, int NWARP, int COLS>
+// NCW consumer warps share a tile of 128 rows x TX_ columns.
+template <typename T, int H, int NCW, int TX_>
 struct TileShape {
     static constexpr int HP = Halo<H>::HP;
-    static constexpr int TX = NWARP * COLS;
+    static constexpr int TX = TX_;
     static constexpr int SZ = kTileZ + 2 * HP;   // rows of the p^n box
     static constexpr int SX = TX + 2 * H;        // columns of the p^n box
     static constexpr int PC_BYTES = SZ * SX * (int)sizeof(T);
@@ -340,6 +343,9 @@ struct ColumnMath {
 #pragma unroll
             for (int q = 0; q < 4; ++q) zz[4 * g + q] = tt[q];
         }
+        // FP32 with FMA: the explicit fused form of the packed pair path
+        // (column_pair_f32), so every FP32 ring variant computes the same bits.
+        constexpr bool kFused = !EXACT && sizeof(T) == 4;
         T lap[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) lap[q] = A::mul(c0, zz[HP + q]);
@@ -352,15 +358,22 @@ struct ColumnMath {
             for (int q = 0; q < 4; ++q) {
                 const T ax = A::add(xp[q], xm[q]);
                 const T az = A::add(zz[HP + q + k], zz[HP + q - k]);
-                lap[q] = A::add(lap[q], A::add(A::mul((T)cx[k], ax), A::mul((T)cz[k], az)));
+                if constexpr (kFused)
+                    lap[q] = __fmaf_rn((float)cz[k], az, __fmaf_rn((float)cx[k], ax, lap[q]));
+                else
+                    lap[q] = A::add(lap[q], A::add(A::mul((T)cx[k], ax), A::mul((T)cz[k], az)));
             }
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const T w = (T)__fmul_rn(wxv, wz[q]);
             const T prev = A::mul(pp[q], w);
-            const T s = A::add(A::sub(A::mul((T)2, zz[HP + q]), prev), A::mul(vd[q], lap[q]));
-            val[q] = A::mul(s, w);
+            if constexpr (kFused) {
+                val[q] = __fmul_rn(__fmaf_rn(vd[q], lap[q], __fmaf_rn(2.0f, zz[HP + q], -prev)), w);
+            } else {
+                const T s = A::add(A::sub(A::mul((T)2, zz[HP + q]), prev), A::mul(vd[q], lap[q]));
+                val[q] = A::mul(s, w);
+            }
         }
     }
 };
@@ -548,12 +561,294 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
     }
 }
 
+// ------------------------------------------------- paired FP32 arithmetic
+// Two FP32 values per operation.  PK<true> issues one packed sm_100
+// instruction (add/mul/fma .f32x2) per operation; PK<false> issues two scalar
+// __fadd_rn / __fmul_rn / __fmaf_rn.  The IEEE (bit-identical) path uses the
+// scalar form: every operation of the reference is then a separately rounded
+// add or multiply that the optimiser never contracts.  The FMA path uses the
+// packed form.  add and mul are written as PTX with an explicit .rn modifier,
+// which the optimiser does not fuse either.
+template <bool PACK>
+struct PK;
+template <>
+struct PK<true> {
+    static __device__ __forceinline__ float2 add(float2 a, float2 b) {
+        float2 d;
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+            "mov.b64 ra, {%2, %3};\n\t"
+            "mov.b64 rb, {%4, %5};\n\t"
+            "add.rn.f32x2 rd, ra, rb;\n\t"
+            "mov.b64 {%0, %1}, rd;\n\t}"
+            : "=f"(d.x), "=f"(d.y)
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+        return d;
+    }
+    static __device__ __forceinline__ float2 mul(float2 a, float2 b) {
+        float2 d;
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+            "mov.b64 ra, {%2, %3};\n\t"
+            "mov.b64 rb, {%4, %5};\n\t"
+            "mul.rn.f32x2 rd, ra, rb;\n\t"
+            "mov.b64 {%0, %1}, rd;\n\t}"
+            : "=f"(d.x), "=f"(d.y)
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+        return d;
+    }
+    static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+};
+template <>
+struct PK<false> {
+    static __device__ __forceinline__ float2 add(float2 a, float2 b) {
+        return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+    }
+    static __device__ __forceinline__ float2 mul(float2 a, float2 b) {
+        return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+    }
+    static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) {
+        return make_float2(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y));
+    }
+};
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// One pair of adjacent columns (a, b = a + 1) of 4 rows per lane, FP32: the
+// Laplacian and the leapfrog update with the sponge, before injection and
+// masking.  The two columns share their x-neighbour loads: the box columns
+// a-H .. b+H are each read once (2H loads for the pair instead of 4H), and the
+// rows are processed two at a time (q = 0,1 and 2,3).
+//
+// EXACT: every operation is a separately rounded IEEE add or multiply in the
+// reference's order (lap = c0 p; lap += cx (xp + xm) + cz (zp + zm) for k = 1..H;
+// p' = w ((2p - w pp) + vd lap)).  Otherwise the same scheme with fused
+// multiply-adds (lap = fma(cz, zp + zm, fma(cx, xp + xm, lap)); p' = w fma(vd,
+// lap, fma(2, p, -w pp))), two rows per packed instruction.  unitw: every cell of the tile has
+// sponge weight exactly 1, so the weight multiplies are the identity and are
+// skipped (bit-identical).
+template <int H, bool EXACT, int SZ, int HP>
+__device__ __forceinline__ void column_pair_f32(const float* ca, const float* ppa_s, const float* vda_s, float wxa,
+                                                float wxb, const float (&wz)[4], float c0, const float* cxs,
+                                                const float* czs, bool unitw, float (&va)[4], float (&vb)[4]) {
+    using P = PK<!EXACT>;
+    constexpr int NZ = 4 + 2 * HP;   // rows of a column window: HP above, 4 own, HP below
+    const float* cb = ca + SZ;
+    float za[NZ], zb[NZ];
+#pragma unroll
+    for (int g = 0; g < NZ / 4; ++g) {
+        ld4(ca - HP + 4 * g, *reinterpret_cast<float(*)[4]>(za + 4 * g));
+        ld4(cb - HP + 4 * g, *reinterpret_cast<float(*)[4]>(zb + 4 * g));
+    }
+    float2 la[2], lb[2];
+    const float2 c0p = dup2(c0);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        la[h] = P::mul(c0p, make_float2(za[HP + 2 * h], za[HP + 2 * h + 1]));
+        lb[h] = P::mul(c0p, make_float2(zb[HP + 2 * h], zb[HP + 2 * h + 1]));
+    }
+    // x queue: L = column a-(k-1), R = column b+(k-1); they start at the centres
+    float L[4], R[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { L[q] = za[HP + q]; R[q] = zb[HP + q]; }
+#pragma unroll
+    for (int k = 1; k <= H; ++k) {
+        float Lk[4], Rk[4];
+        ld4(ca - k * SZ, Lk);
+        ld4(cb + k * SZ, Rk);
+        const float2 cxp = dup2(cxs[k]), czp = dup2(czs[k]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = HP + 2 * h;   // first of the two rows of this pair
+            // column a: x-k = Lk, x+k = R;  column b: x-k = L, x+k = Rk
+            const float2 axa = P::add(make_float2(R[2 * h], R[2 * h + 1]), make_float2(Lk[2 * h], Lk[2 * h + 1]));
+            const float2 axb = P::add(make_float2(Rk[2 * h], Rk[2 * h + 1]), make_float2(L[2 * h], L[2 * h + 1]));
+            float2 aza, azb;
+            if ((k & 1) == 0) {   // rows r+-k, r+1+-k are aligned register pairs
+                aza = P::add(make_float2(za[r + k], za[r + 1 + k]), make_float2(za[r - k], za[r + 1 - k]));
+                azb = P::add(make_float2(zb[r + k], zb[r + 1 + k]), make_float2(zb[r - k], zb[r + 1 - k]));
+            } else {              // odd shift: form the sums from single rows
+                aza = make_float2(__fadd_rn(za[r + k], za[r - k]), __fadd_rn(za[r + 1 + k], za[r + 1 - k]));
+                azb = make_float2(__fadd_rn(zb[r + k], zb[r - k]), __fadd_rn(zb[r + 1 + k], zb[r + 1 - k]));
+            }
+            if (EXACT) {
+                la[h] = P::add(la[h], P::add(P::mul(cxp, axa), P::mul(czp, aza)));
+                lb[h] = P::add(lb[h], P::add(P::mul(cxp, axb), P::mul(czp, azb)));
+            } else {
+                la[h] = P::fma(czp, aza, P::fma(cxp, axa, la[h]));
+                lb[h] = P::fma(czp, azb, P::fma(cxp, axb, lb[h]));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { L[q] = Lk[q]; R[q] = Rk[q]; }
+    }
+    // p' = w ((2p - w pp) + vd lap); p^{n-1} and (v dt)^2 of the pair are read
+    // only now (column b follows column a at kTileZ floats in both boxes)
+    float ppa[4], ppb[4], vda[4], vdb[4];
+    ld4(ppa_s, ppa);
+    ld4(ppa_s + kTileZ, ppb);
+    ld4(vda_s, vda);
+    ld4(vda_s + kTileZ, vdb);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float2 wzp = make_float2(wz[2 * h], wz[2 * h + 1]);
+        const float2 pa = make_float2(za[HP + 2 * h], za[HP + 2 * h + 1]);
+        const float2 pb = make_float2(zb[HP + 2 * h], zb[HP + 2 * h + 1]);
+        const float2 ppa2 = make_float2(ppa[2 * h], ppa[2 * h + 1]);
+        const float2 ppb2 = make_float2(ppb[2 * h], ppb[2 * h + 1]);
+        const float2 vda2 = make_float2(vda[2 * h], vda[2 * h + 1]);
+        const float2 vdb2 = make_float2(vdb[2 * h], vdb[2 * h + 1]);
+        float2 ra, rb;
+        if (unitw) {
+            if (EXACT) {
+                ra = P::add(P::add(P::add(pa, pa), neg2(ppa2)), P::mul(vda2, la[h]));
+                rb = P::add(P::add(P::add(pb, pb), neg2(ppb2)), P::mul(vdb2, lb[h]));
+            } else {
+                ra = P::fma(vda2, la[h], P::fma(dup2(2.0f), pa, neg2(ppa2)));
+                rb = P::fma(vdb2, lb[h], P::fma(dup2(2.0f), pb, neg2(ppb2)));
+            }
+        } else {
+            const float2 wa = P::mul(dup2(wxa), wzp), wb = P::mul(dup2(wxb), wzp);
+            if (EXACT) {
+                ra = P::mul(P::add(P::add(P::add(pa, pa), neg2(P::mul(ppa2, wa))), P::mul(vda2, la[h])), wa);
+                rb = P::mul(P::add(P::add(P::add(pb, pb), neg2(P::mul(ppb2, wb))), P::mul(vdb2, lb[h])), wb);
+            } else {
+                ra = P::mul(P::fma(vda2, la[h], P::fma(dup2(2.0f), pa, neg2(P::mul(ppa2, wa)))), wa);
+                rb = P::mul(P::fma(vdb2, lb[h], P::fma(dup2(2.0f), pb, neg2(P::mul(ppb2, wb)))), wb);
+            }
+        }
+        va[2 * h] = ra.x; va[2 * h + 1] = ra.y;
+        vb[2 * h] = rb.x; vb[2 * h + 1] = rb.y;
+    }
+}
+
+// Which of a tile's work items (column pairs, or passes of packed columns) the
+// consumer warp `warp` takes first: items go round-robin over the NCW warps
+// from a first warp that moves with the tile's position, so that the warps that
+// get one item more than the others change from tile to tile.
+template <int NCW>
+__device__ __forceinline__ int first_item(const TileInfo& t, int tx, int warp) {
+    const int j = (int)(((unsigned)t.x0 / (unsigned)tx + (unsigned)t.tz) % NCW);
+    const int f = warp - j;
+    return f < 0 ? f + NCW : f;
+}
+
+// Full bands (32 lanes per column, the common case) of an FP32 tile: the tile's
+// TX/2 pairs of adjacent columns go round-robin to the consumer warps; the two
+// columns of a pair share their x-neighbour loads (column_pair_f32); the
+// epilogue is the shared per-column one.
+template <int H, bool EXACT, int NCW, int TX>
+__device__ __forceinline__ void compute_tile_full_f32(const unsigned char* __restrict__ st, const TileInfo& t,
+                                                      float* __restrict__ pcur, float* __restrict__ pnext,
+                                                      int ldz) {
+    using S = TileShape<float, H, NCW, TX>;
+    constexpr int HP = S::HP;
+    const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
+    const float* __restrict__ sm_pc = reinterpret_cast<const float*>(st + S::PC_OFF);
+    const float* __restrict__ sm_pp = reinterpret_cast<const float*>(st + S::PP_OFF);
+    const float* __restrict__ sm_vd = reinterpret_cast<const float*>(st + S::VD_OFF);
+    const float* __restrict__ sm_wx = reinterpret_cast<const float*>(st + S::WX_OFF);
+    const float* __restrict__ sm_wz = reinterpret_cast<const float*>(st + S::WZ_OFF);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nb = d.nb, nx = d.nx, lds = d.lds, zs0 = d.zs0;
+    const int zr = t.z0 + 4 * lane;
+    const bool lane_in = zr < d.nze;
+    const bool lane_snap = lane_in && zr >= zs0 && zr < zs0 + lds;
+    const bool first = t.first;
+    const bool do_image = t.do_image;
+    const bool unitw = t.unitw;
+    float wz[4];
+    {
+        const float4 w4 = *reinterpret_cast<const float4*>(sm_wz + 4 * lane);
+        wz[0] = w4.x; wz[1] = w4.y; wz[2] = w4.z; wz[3] = w4.w;
+    }
+    // Pairs of this warp: f, f + NCW, ... (a compile-time count when the
+    // tile's pairs divide evenly over the warps).
+    constexpr int kPairs = TX / 2;
+    constexpr int kEven = kPairs % NCW == 0 ? kPairs / NCW : 0;
+    const int f = first_item<NCW>(t, TX, warp);
+    const int npr = kEven ? kEven : (kPairs - f + NCW - 1) / NCW;
+
+    // Plain tile on an unstored step (most of the work): every cell is live,
+    // inside the zero ring and free of injection and recording, so each pair
+    // is computed and stored with nothing else.
+    if (t.plain && !t.do_snap && !do_image) {
+#pragma unroll
+        for (int i = 0; i < (kEven ? kEven : 1); ++i) {
+            for (int j = 0; j < (kEven ? 1 : npr); ++j) {
+                const int la = 2 * (f + (i + j) * NCW);
+                float va[4], vb[4];
+                float* dst = pnext + (uint32_t)(t.x0 + la) * (uint32_t)ldz + zr;
+                if (first) {
+                    const float z4[4] = {0.f, 0.f, 0.f, 0.f};
+                    float* cur = pcur + (uint32_t)(t.x0 + la) * (uint32_t)ldz + zr;
+                    stg4(dst, z4);
+                    stg4(dst + ldz, z4);
+                    stg4(cur, z4);
+                    stg4(cur + ldz, z4);
+                } else {
+                    column_pair_f32<H, EXACT, S::SZ, HP>(sm_pc + (la + H) * S::SZ + 4 * lane + HP,
+                                                          sm_pp + la * kTileZ + 4 * lane,
+                                                          sm_vd + la * kTileZ + 4 * lane, sm_wx[la], sm_wx[la + 1],
+                                                          wz, d.c0, d.cx, d.cz, unitw, va, vb);
+                    stg4(dst, va);
+                    stg4(dst + ldz, vb);
+                }
+            }
+        }
+        return;
+    }
+
+    for (int j = 0; j < npr; ++j) {
+        const int la = 2 * (f + j * NCW);
+        float va[4], vb[4];
+        if (first) {
+            // p^n = p^{n-1} = 0 on the first step of a pass: the update is +0
+            // in every rounding step, and the boxes were not loaded.
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { va[q] = 0.f; vb[q] = 0.f; }
+        } else {
+            column_pair_f32<H, EXACT, S::SZ, HP>(sm_pc + (la + H) * S::SZ + 4 * lane + HP,
+                                                  sm_pp + la * kTileZ + 4 * lane, sm_vd + la * kTileZ + 4 * lane,
+                                                  sm_wx[la], sm_wx[la + 1], wz, d.c0, d.cx, d.cz, unitw, va, vb);
+        }
+        const RecEntry* re = reinterpret_cast<const RecEntry*>(st + S::REC_OFF);
+        const int* off = t.has_pts
+                             ? reinterpret_cast<const int*>(st + (t.rec_staged ? S::RCS_OFF : S::CS_OFF))
+                             : nullptr;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int lx = la + c, x = t.x0 + lx;
+            float vd[4], fs[4], Iv[4], Sv[4];
+            ld4(sm_vd + lx * kTileZ + 4 * lane, vd);   // injection weights (the epilogue's only use)
+            if (do_image && lane_snap && x >= nb && x < nb + nx) {
+                const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
+                const size_t cell = (size_t)t.ksnap * nx * lds + ic;
+                const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
+                load_snapshot4<float>(d, cell, eidx, fs);
+                ldg4(reinterpret_cast<const float*>(d.img) + ic, Iv, 0);
+                ldg4(reinterpret_cast<const float*>(d.ill) + ic, Sv, 0);
+            }
+            column_epilogue<float, H, EXACT>(d, t, x, zr, lane, lane_in, lane_snap, c ? vb : va, vd, fs, Iv, Sv,
+                                             off ? off[lx] : 0, off ? off[lx + 1] : 0, re, pcur, pnext, ldz, 32);
+        }
+    }
+}
+
 // ------------------------------------------------------------- the tile
 // Computes one tile after its boxes have landed in the stage.
-template <typename T, int H, bool EXACT, int NWARP, int COLS>
+template <typename T, int H, bool EXACT, int NCW, int TX>
 __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ st, const TileInfo& t,
                                              T* __restrict__ pcur, T* __restrict__ pnext, int ldz) {
-    using S = TileShape<T, H, NWARP, COLS>;
+    // FP32 full bands take the column-pair path, except in the 8-warp x
+    // 16-column shape: it runs 2 CTAs of 9 warps per SM at 96 registers per
+    // thread, where the per-column path below fits without spilling.
+    if constexpr (sizeof(T) == 4 && !(NCW == 8 && TX == 16)) {
+        if (t.glog == 5) {   // full band: the column-pair path
+            compute_tile_full_f32<H, EXACT, NCW, TX>(st, t, pcur, pnext, ldz);
+            return;
+        }
+    }
+    using S = TileShape<T, H, NCW, TX>;
     constexpr int HP = S::HP;
     const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
     const T* __restrict__ sm_pc = reinterpret_cast<const T*>(st + S::PC_OFF);
@@ -570,10 +865,9 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
 
     // A band with few live rows (the last band of a shot) packs several columns
     // into one warp: G = 2^t.glog lanes per column (set by the producer) and
-    // 32 / G columns per pass.  Passes go round-robin over the warps from a
-    // first warp that moves with the tile's x position, so that the packed
-    // bands of successive tiles land on different warps.  G = 32 is one column
-    // per pass.
+    // 32 / G columns per pass.  Passes go round-robin over the consumer warps
+    // (first_item), so that the packed bands of successive tiles land on
+    // different warps.  G = 32 is one column per pass.
     const int lg = t.glog;
     const int G = 1 << lg;
     const int cpp = 32 >> lg;
@@ -592,11 +886,13 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
         wz[0] = w4.x; wz[1] = w4.y; wz[2] = w4.z; wz[3] = w4.w;
     }
 
+    const int npass = TX / cpp;
+    const int f = first_item<NCW>(t, TX, warp);
 #pragma unroll
-    for (int c = 0; c < COLS; ++c) {
-        const int base = (c * NWARP + (warp + (unsigned)t.x0 / S::TX) % NWARP) * cpp;
-        if (base >= S::TX) continue;             // warp-uniform
-        const int lx = base + (lane >> lg);
+    for (int c = 0; c < (TX + NCW - 1) / NCW; ++c) {
+        const int ps = f + c * NCW;
+        if (ps >= npass) continue;               // warp-uniform
+        const int lx = ps * cpp + (lane >> lg);
         const int x = t.x0 + lx;
         const T* col = sm_pc + (lx + H) * S::SZ + 4 * sub + HP;   // row zr of column x
         const bool col_int = (x >= nb) && (x < nb + nx);
@@ -758,11 +1054,11 @@ __device__ __forceinline__ bool stage_receivers(const ShotDesc& sd, const TileIn
 // are issued in as few dependent rounds as possible: the descriptor words and
 // both tapers first (before the TMA issue, so their latency overlaps it), the
 // receiver tables after the descriptor has reached shared memory.
-template <typename T, int H, int NWARP, int COLS>
+template <typename T, int H, int NCW, int TX>
 __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, const CUtensorMap* map_pc,
                                              const CUtensorMap* map_box, const StepParams& p, const TileRef& tr,
                                              long long g) {
-    using S = TileShape<T, H, NWARP, COLS>;
+    using S = TileShape<T, H, NCW, TX>;
     static_assert(S::TX <= 32, "one producer lane per tile column");
     static_assert(kTileZ == 4 * 32, "one float4 of the z taper per producer lane");
     static_assert((S::TX & (S::TX - 1)) == 0, "tile width is a power of two");
@@ -803,6 +1099,15 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
     const float wxv = (lane < S::TX && xw < nxe) ? __ldg(tr.wx + xw) : 0.f;
     float4 wzv = make_float4(0.f, 0.f, 0.f, 0.f);
     if (z0 + 4 * lane < tr.nze) wzv = __ldg(reinterpret_cast<const float4*>(tr.wz + z0 + 4 * lane));
+    // Sponge weight exactly 1 on every live cell of the tile (its live columns
+    // and rows): the consumers then skip the weight multiplies.
+    {
+        const int zl = z0 + 4 * lane;
+        const bool xok = lane >= S::TX || xw >= nxe || wxv == 1.0f;
+        const bool zok = (zl >= tr.nze || wzv.x == 1.0f) && (zl + 1 >= tr.nze || wzv.y == 1.0f) &&
+                         (zl + 2 >= tr.nze || wzv.z == 1.0f) && (zl + 3 >= tr.nze || wzv.w == 1.0f);
+        ti.unitw = __all_sync(0xffffffffu, xok && zok) ? 1 : 0;
+    }
 
     if (lane == 0) {
         *reinterpret_cast<TileInfo*>(st + S::INFO_OFF) = ti;
@@ -867,16 +1172,19 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
 
 // ------------------------------------------------------- per-step kernel
 // One launch = one time step of every tile in the tile list.  Persistent and
-// warp-specialised: warp NWARP is the producer, which walks the CTA's tiles
+// warp-specialised: warp NCW is the producer, which walks the CTA's tiles
 // (stride gridDim.x) and fills a ring of `nstage` shared-memory stages; warps
-// 0..NWARP-1 are consumers that compute each tile as soon as its stage is full
+// 0..NCW-1 are consumers that compute each tile as soon as its stage is full
 // and release it.  No CTA-wide barrier inside the loop: the producer runs up to
 // nstage-1 tiles ahead of the consumers, so TMA latency hides behind compute.
-template <typename T, int H, bool EXACT, int NWARP, int COLS>
-__global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
+//
+// The CTAs per SM of each shape (and so its register budget) are those of
+// step_ctas_per_sm in kernels.hpp.
+template <typename T, int H, bool EXACT, int NCW, int TX>
+__global__ void __launch_bounds__((NCW + 1) * 32, sizeof(T) == 8 ? 1 : (NCW == 4 ? 3 : (TX == 16 ? 2 : 1)))
     step_kernel(const __grid_constant__ CUtensorMap map_pc, const __grid_constant__ CUtensorMap map_box,
                 const StepParams p) {
-    using S = TileShape<T, H, NWARP, COLS>;
+    using S = TileShape<T, H, NCW, TX>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
     uint64_t* empty = full + kMaxStages;
@@ -889,7 +1197,7 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
     if (threadIdx.x == 0) {
         for (int s = 0; s < nst; ++s) {
             mbar_init(full + s, 32);
-            mbar_init(empty + s, NWARP * 32);
+            mbar_init(empty + s, NCW * 32);
             issued[s] = 0;
         }
         *abort_flag = 0;
@@ -901,7 +1209,7 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
     const long long g = *p.step_counter + p.step_offset;
     const int warp = threadIdx.x >> 5;
 
-    if (warp == NWARP) {
+    if (warp == NCW) {
         int s = 0, round = 0;   // stage and how many times the ring has wrapped
         TileRef cur = p.tiles[blockIdx.x];
         TileRef nxt = cur;
@@ -911,7 +1219,7 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
             // Failure-detection test: a tile whose stage is never filled makes the
             // consumers' bounded wait run out (no copy is in flight for it).
             if (t != p.stall_tile) {
-                produce_tile<T, H, NWARP, COLS>(stages + (size_t)s * S::STAGE, full + s, &map_pc, &map_box, p, cur,
+                produce_tile<T, H, NCW, TX>(stages + (size_t)s * S::STAGE, full + s, &map_pc, &map_box, p, cur,
                                                 g);
                 if ((threadIdx.x & 31) == 0) issued[s] = round + 1;
             }
@@ -928,7 +1236,7 @@ __global__ void __launch_bounds__((NWARP + 1) * 32, sizeof(T) == 8 ? 1 : 2)
             if (info.active) {
                 const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
                 T* base = reinterpret_cast<T*>(p.fields) + (size_t)d.field_slot * p.slot_stride;
-                compute_tile<T, H, EXACT, NWARP, COLS>(st, info, base + (size_t)info.cur * p.buf_stride,
+                compute_tile<T, H, EXACT, NCW, TX>(st, info, base + (size_t)info.cur * p.buf_stride,
                                                        base + (size_t)(info.cur ^ 1) * p.buf_stride, p.ldz);
             }
             mbar_arrive(empty + s);

@@ -31,7 +31,7 @@ static void usage() {
         "  --illumination  --filter laplacian  --write-illum-map\n"
         "  --benchmark PATH  --benchmark-csv PATH  --dataset NAME\n"
         "  --segy-src-depth M (10)  --segy-rec-depth M (10)  --quiet\n"
-        "  --snap-precision f32|bf16|f16  --arith ieee|fma|fp64  --max-in-flight N  --tile-cols 0|16|32\n"
+        "  --snap-precision f32|bf16|f16  --arith auto|ieee|fma|fp64  --max-in-flight N  --tile-cols 0|16|32\n"
         "  --check-inputs         read and validate the inputs, print a summary, exit\n");
 }
 
@@ -93,7 +93,8 @@ int main(int argc, char** argv) try {
             if (v == "ieee") opt.arithmetic = RTM_B200_ARITH_IEEE;
             else if (v == "fma") opt.arithmetic = RTM_B200_ARITH_FMA;
             else if (v == "fp64") opt.arithmetic = RTM_B200_ARITH_FP64;
-            else throw std::runtime_error("--arith ieee|fma|fp64");
+            else if (v == "auto") opt.arithmetic = RTM_B200_ARITH_AUTO;
+            else throw std::runtime_error("--arith auto|ieee|fma|fp64");
         } else if (a == "--max-in-flight") opt.max_shots_in_flight = std::stoi(next());
         else if (a == "--tile-cols") opt.tile_cols = std::stoi(next());
         else if (a == "--check-inputs") check_only = true;

@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", 
 
 MODE_PLAIN, MODE_BATCH, MODE_SERVE = 0, 1, 2
 SNAP_F32, SNAP_BF16, SNAP_F16 = 0, 1, 2
-ARITH_IEEE, ARITH_FMA, ARITH_FP64 = 0, 1, 2
+ARITH_IEEE, ARITH_FMA, ARITH_FP64, ARITH_AUTO = 0, 1, 2, 3
 ACC_PLAIN, ACC_COMPENSATED = 0, 1
 
 

@@ -87,7 +87,7 @@ def shots_to_c(shots: Sequence[ShotRecord], keep: list):
 
 _MODES = {"plain": L.MODE_PLAIN, "batch": L.MODE_BATCH, "serve": L.MODE_SERVE}
 _SNAPS = {"f32": L.SNAP_F32, "bf16": L.SNAP_BF16, "f16": L.SNAP_F16}
-_ARITH = {"ieee": L.ARITH_IEEE, "fma": L.ARITH_FMA, "fp64": L.ARITH_FP64}
+_ARITH = {"ieee": L.ARITH_IEEE, "fma": L.ARITH_FMA, "fp64": L.ARITH_FP64, "auto": L.ARITH_AUTO}
 _ACC = {"plain": L.ACC_PLAIN, "compensated": L.ACC_COMPENSATED}
 
 
@@ -95,7 +95,7 @@ class Engine:
     """A B200 RTM engine (one CUDA device, one host thread at a time)."""
 
     def __init__(self, mode: str = "plain", params: Optional[RTMParams] = None, *, snap: str = "f32",
-                 arithmetic: str = "ieee", accumulation: str = "compensated", device: int = 0,
+                 arithmetic: str = "auto", accumulation: str = "compensated", device: int = 0,
                  max_shots_in_flight: int = 0, device_mem_budget: int = 0, tile_cols: int = 0,
                  chunk_steps: int = 0, serve_max_nx: int = 0, serve_max_nz: int = 0):
         self.lib = L.load()
