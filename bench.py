@@ -2,37 +2,47 @@
 """Benchmark of the B200 RTM engine (one JSON line on stdout, rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload config3|config2|config1|config4|config5]
 
-Workload (default): 1150 x 400 cells at 10 m, layered-and-faulted velocity
-1500-5500 m/s (10 dipping interfaces, 3 normal faults, seed 2), 64 shots with a
-split-spread line of receivers on every column, nt 4000, dt 0.8 ms, Ricker 15
-Hz, order 8, nb 60, store interval 2.  Traces are modelled on the GPU with the
-same scheme before timing (synthetic data; the reference's own synthetic data is
-made the same way).  One step = one full migration of the shot set.
+Contract line (default, --workload config3): the batched-shot survey.  1150 x
+400 cells at 10 m, seeded layered-and-faulted velocity 1500-5500 m/s; 256 shots
+per GPU, each migrated on its own aperture window of uniform random width
+400-1150 columns (seed 3) with receivers on every window column; nt 4000, dt
+0.8 ms, Ricker 15 Hz, order 8, nb 60, store interval 2.  Traces are modelled on
+the GPU with the same scheme before timing (the reference makes its synthetic
+data the same way).  One step = one migration of the GPU's 256 shots by the
+batched engine with BF16 snapshots (power-of-two scale per 128-row column
+segment), compensated FP32 per-shot sums and the FP64 cross-shot stack; with
+N > 1 GPUs the step ends with the one exchange of the path, an all-reduce of the
+FP64 stacks.
 
-value      shots/s with the shot gathers already resident in HBM (device time,
-           CUDA events on the engine's stream, max over ranks);
-e2e        shots/s through the C ABI with page-locked HOST traces and host
-           outputs, the host->device copies inside the timed region;
-roofline   algorithmic bytes of the step kernel (16 B per cell update, snapshot
-           stores and reloads, image/illumination read+write, traces) per
-           second of device time, against the measured HBM copy bandwidth;
-cpu_baseline  the reference's own CPU engine (oracle/_ref/rtm, engine cpu-opt,
-           all host cores) on one shot with a truncated time axis, extrapolated
-           per cell update.
+value        shots/s with the gathers resident in HBM: device time (CUDA events
+             on the engine's stream, plus the all-reduce on N > 1), max over
+             ranks;
+e2e          shots/s through the C ABI with page-locked HOST gathers and host
+             outputs, the host<->device copies inside the timed region;
+roofline     algorithmic bytes of the step kernel per second of device time
+             against the measured HBM copy bandwidth (the fields of the shots in
+             flight exceed L2);
+plain_f32    the plain FP32 engine (one shot at a time, bit-identical to the
+             reference CPU engine) on the same shots, its roofline against the
+             L2 copy bandwidth (its fields are L2-resident), and the ratio;
+cpu_baseline the reference's own CPU engine (oracle/_ref/rtm, cpu-opt, all host
+             cores) migrating one whole shot of the survey.
 
---impl reference runs only that reference CPU engine (rank 0), one bounded
-sample per step.  Multi-GPU (torchrun): shots are sharded across ranks (each
-rank migrates a fixed 64-shot share: weak scaling) and the FP64 image stacks are
-summed with one NCCL all-reduce at the end of each step.
+--impl reference times that reference CPU engine alone (rank 0 only), one whole
+shot of the survey per step.  --workload config2/config1/config4/config5 print
+the other configurations' lines.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import shutil
 import statistics
+import struct
 import subprocess
 import sys
 import tempfile
@@ -40,36 +50,43 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(ROOT, "rtm-acceleration_b200"))
+PKG = os.path.join(ROOT, "rtm-acceleration_b200")
+sys.path.insert(0, PKG)
 
 import numpy as np  # noqa: E402
 
-SHOTS_PER_GPU = 64
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 TRAFFIC_PATH = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+REF_RTM = os.path.join(ROOT, "oracle", "_ref", "rtm")
+REF_BUILD = ("reference sources compiled by oracle/Makefile: engine cpu-opt at -O3 -march=x86-64-v3 "
+             "-ffp-contract=off -fopenmp (the reference's CMake uses -march=native; x86-64-v3 keeps the binary "
+             "portable to the GPU box's host)")
 
 
-def parse_args():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU, help="shots per GPU")
-    ap.add_argument("--nt", type=int, default=0, help="override nt (0 = 4000)")
+    ap.add_argument("--workload", default="config3", choices=["config1", "config2", "config3", "config4", "config5"])
+    ap.add_argument("--shots", type=int, default=0, help="shots per GPU (0: 256 for config3, 64 for config2)")
+    ap.add_argument("--nt", type=int, default=0, help="override nt (0: the config's)")
+    ap.add_argument("--order", type=int, default=8)
     ap.add_argument("--mode", default="batch", choices=["batch", "plain"])
-    ap.add_argument("--max-in-flight", type=int, default=0, help="0 = the engine's default (16)")
-    ap.add_argument("--tile-cols", type=int, default=0, help="0 = autotuned")
-    ap.add_argument("--snap", default="f32", choices=["f32", "bf16", "f16"])
+    ap.add_argument("--snap", default="", choices=["", "f32", "bf16", "f16"],
+                    help="snapshot precision ('': bf16 for config3, f32 for config2)")
     ap.add_argument("--arith", default="auto", choices=["auto", "ieee", "fma"])
+    ap.add_argument("--max-in-flight", type=int, default=0, help="0 = the engine's choice")
+    ap.add_argument("--tile-cols", type=int, default=0, help="0 = autotuned")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="timed steps of the e2e leg (at most --steps)")
+    ap.add_argument("--plain-shots", type=int, default=0, help="shots timed on the plain engine (0 = all)")
     ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
-                    help="config2 is the contract line; the others print one extra JSON line each")
-    ap.add_argument("--plain-shots", type=int, default=64, help="config3: shots timed on the plain engine")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain engine and order-12 legs")
     ap.add_argument("--requests", type=int, default=24, help="config5: requests in the stream")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ------------------------------------------------------------------ clocks
@@ -118,35 +135,7 @@ class ClockSampler:
                 "samples": len(load)}
 
 
-# ---------------------------------------------------------------- workload
-def make_workload(nshots_total, nt_override):
-    from rtm_b200 import synth
-    w = synth.config2(nshots=nshots_total)
-    if nt_override:
-        w.nt = nt_override
-        for s in w.shots:
-            s.nt = nt_override
-    return w
-
-
-def model_traces(w, device):
-    from rtm_b200 import Engine, RTMParams
-    p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=1)
-    with Engine("batch", p, device=device, max_shots_in_flight=16) as e:
-        e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-        tr = e.model_shots(w.shots)
-    for s, t in zip(w.shots, tr):
-        s.traces = t
-
-
-def algorithmic_bytes_per_shot(w, snap_bytes):
-    """16 B per cell update + snapshot store/reload + image/illum RMW + traces."""
-    nsnap = (w.nt - 1) // w.store_interval + 1
-    nint = w.nx * w.nz
-    upd = 2.0 * w.nt * (w.nx + 2 * w.nb) * (w.nz + 2 * w.nb)
-    return 16.0 * upd + nsnap * nint * snap_bytes + nsnap * nint * (snap_bytes + 16.0) + w.nx * w.nt * 4.0
-
-
+# ------------------------------------------------------------ peaks, bytes
 def read_peak():
     try:
         with open(PEAKS_PATH) as f:
@@ -163,241 +152,141 @@ def read_traffic():
         return None
 
 
-# ------------------------------------------------------------ reference CPU
-def reference_sample(w, workdir, nt_sample, threads):
-    """Time the reference's cpu-opt engine on one config shot with a truncated
-    time axis; returns (cell_updates_per_s, seconds, description)."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "rtm")
-    if not os.path.exists(ref):
-        return None
-    from rtm_b200 import io as rio
-    vel = os.path.join(workdir, "velocity.bin")
-    rio.write_velocity_raw(vel, w.vel)
-    rio.write_header_file(vel + ".hdr", rio.VelocityHeader(w.nx, w.nz, w.dx, w.dz, 0.0, 0.0, "zfast"))
-    s0 = w.shots[len(w.shots) // 2]
-    rng = np.random.default_rng(7)
-    from rtm_b200.engine import ShotRecord
-    sh = ShotRecord(s0.sx, s0.sz, s0.rx, s0.rz, nt=nt_sample, dt=w.dt,
-                    traces=(rng.standard_normal(s0.nrec * nt_sample) * 1e-3).astype(np.float32))
-    shots_path = os.path.join(workdir, "shots.bin")
-    rio.write_shots_raw(shots_path, [sh])
-    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    cmd = [ref, "--engine", "cpu-opt", "--velocity", vel, "--shots", shots_path, "--output",
-           os.path.join(workdir, "img.bin"), "--order", str(w.order), "--nb", str(w.nb), "--f0", str(w.f0),
-           "--store-interval", str(w.store_interval), "--quiet"]
+def algorithmic_bytes(w, shots, snap_bytes):
+    """Bytes the roofline counts per migration of `shots` (summed): 16 B per cell
+    update (read p^n, p^{n-1}, (v dt)^2; write p^{n+1}), the snapshot store, the
+    stored backward steps (snapshot read, image and illumination read+write) and
+    the traces.  Compensation words are overhead, not counted."""
+    nsnap = (w.nt - 1) // w.store_interval + 1
+    tot = 0.0
+    for s in shots:
+        wx = s.window_nx or w.nx
+        upd = 2.0 * w.nt * (wx + 2 * w.nb) * (w.nz + 2 * w.nb)
+        nint = wx * w.nz
+        tot += 16.0 * upd + nsnap * nint * snap_bytes + nsnap * nint * (snap_bytes + 16.0) + s.nrec * w.nt * 4.0
+    return tot
+
+
+def stencil_bytes(w, shots):
+    """The 16 B per cell update part alone (the L2-resident traffic of the plain engine)."""
+    return sum(16.0 * 2.0 * w.nt * ((s.window_nx or w.nx) + 2 * w.nb) * (w.nz + 2 * w.nb) for s in shots)
+
+
+def cell_updates(w, shots):
+    return sum(2.0 * w.nt * ((s.window_nx or w.nx) + 2 * w.nb) * (w.nz + 2 * w.nb) for s in shots)
+
+
+# --------------------------------------------- the reference's CPU engine
+def _velocity_models():
+    """rtm_b200/velocity_models.py loaded on its own (numpy only): the reference
+    arm builds the same models without importing the engine package."""
+    spec = importlib.util.spec_from_file_location("rtm_velocity_models",
+                                                  os.path.join(PKG, "rtm_b200", "velocity_models.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _write_velocity(path, v_zfast, nx, nz, d, ox):
+    np.ascontiguousarray(v_zfast, "<f4").tofile(path)
+    with open(path + ".hdr", "w") as f:
+        f.write(f"nx = {nx}\nnz = {nz}\ndx = {d:g}\ndz = {d:g}\nox = {ox:g}\noz = 0\nlayout = zfast\n")
+
+
+def _write_rtms(path, sx, rx, nt, dt, traces):
+    """One-shot RTMS v1 file (the reference's raw shot format)."""
+    nrec = rx.size
+    with open(path, "wb") as f:
+        f.write(b"RTMS" + struct.pack("<4if2i", 1, 1, nrec, nt, np.float32(dt), 0, 0))
+        f.write(struct.pack("<2f", sx, 0.0))
+        f.write(np.ascontiguousarray(rx, "<f4").tobytes())
+        f.write(np.zeros(nrec, "<f4").tobytes())
+        f.write(np.ascontiguousarray(traces, "<f4").tobytes())
+
+
+def config3_reference_shot(vm, v_full, i, nshots=256, nx=1150, nz=400, d=10.0, nt=4000):
+    """Inputs of survey shot i for the reference CLI, which has no aperture
+    windows: the window's columns as their own velocity file (origin ox = x0 dx),
+    the shot in the model's metres, seeded random traces (the CPU time does not
+    depend on trace values)."""
+    x0, w = vm.config3_windows(nshots, nx)[i % nshots]
+    v = np.asarray(v_full, np.float32).reshape(nx, nz)[x0:x0 + w].ravel()
+    rx = (np.arange(x0, x0 + w, dtype=np.float32) * np.float32(d)).astype(np.float32)
+    sx = float(np.float32((x0 + w // 2) * d))
+    tr = (np.random.default_rng(100 + i).standard_normal(w * nt) * 1e-3).astype(np.float32)
+    return v, w, x0 * d, sx, rx, tr
+
+
+def time_reference_shot(td, vm, v_full, i, order, threads, nt=4000, dt=0.0008):
+    """Wall time of the reference's cpu-opt engine migrating survey shot i whole
+    (process start, file reads and the image write included)."""
+    v, w, ox, sx, rx, tr = config3_reference_shot(vm, v_full, i, nt=nt)
+    vel, shp = os.path.join(td, "v.bin"), os.path.join(td, "s.bin")
+    _write_velocity(vel, v, w, 400, 10.0, ox)
+    _write_rtms(shp, sx, rx, nt, dt, tr)
+    cmd = [REF_RTM, "--engine", "cpu-opt", "--velocity", vel, "--shots", shp, "--output", os.path.join(td, "i.bin"),
+           "--order", str(order), "--nb", "60", "--f0", "15", "--store-interval", "2", "--quiet"]
     t0 = time.perf_counter()
-    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env)
-    dt = time.perf_counter() - t0
-    upd = 2.0 * nt_sample * (w.nx + 2 * w.nb) * (w.nz + 2 * w.nb)
-    desc = (f"reference cpu-opt, 1 shot of the workload with nt truncated to {nt_sample} "
-            f"({upd / 1e9:.2f} G cell updates), {threads} threads, wall time of the rtm process")
-    return upd / dt, dt, desc
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+    sec = time.perf_counter() - t0
+    upd = 2.0 * nt * (w + 120) * (400 + 120)
+    return sec, upd, w
 
 
 def run_reference_arm(args):
+    """The reference's own CPU engine on the survey, one whole shot per step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    w = make_workload(SHOTS_PER_GPU, args.nt)
-    upd_shot = 2.0 * w.nt * (w.nx + 2 * w.nb) * (w.nz + 2 * w.nb)
-    nt_sample = 300
-    ref = os.path.join(ROOT, "oracle", "_ref", "rtm")
-    if not os.path.exists(ref):
+    if args.workload != "config3":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the config3 survey only"}))
+        return
+    if not os.path.exists(REF_RTM):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU engine not built (oracle/_ref/rtm)"}))
         return
-    rates = []
-    desc = ""
+    threads = os.cpu_count() or 1
+    vm = _velocity_models()
+    v_full = vm.layered_faulted(1150, 400, 10.0, 10.0, seed=3)
+    nt = args.nt or 4000
+    secs, upds, widths = [], [], []
     with tempfile.TemporaryDirectory() as td:
         for i in range(args.warmup + args.steps):
-            r = reference_sample(w, td, nt_sample, threads)
+            sec, upd, w = time_reference_shot(td, vm, v_full, i, args.order, threads, nt=nt)
             if i >= args.warmup:
-                rates.append(r[0])
-                desc = r[2]
-    rate = statistics.median(rates)
-    value = rate / upd_shot
+                secs.append(sec)
+                upds.append(upd)
+                widths.append(w)
+    value = len(secs) / sum(secs)
+    sample = (f"reference cpu-opt on {threads} threads, survey shots {args.warmup}..{args.warmup + args.steps - 1} "
+              f"whole (windows {min(widths)}-{max(widths)} columns, nt {nt}), one per step, wall time of the rtm "
+              f"process; random traces; {REF_BUILD}")
     line = {"impl": "reference", "metric": "shots/s", "value": value, "unit": "shots/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * SHOTS_PER_GPU / value,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "gcell_updates_per_s": rate / 1e9,
-            "config": {"workload": "config2: 1150x400 @10 m, 64 shots, nt 4000, order 8, store 2",
-                       "inputs": "random traces, one shot per sample (timing only)"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "gcell_updates_per_s": sum(upds) / sum(secs) / 1e9,
+            "config": {"workload": f"config3: 1150x400 @10 m survey, aperture windows 400-1150 columns, nt {nt}, "
+                                   f"order {args.order}, store 2, one whole shot per step"},
             "cpu_baseline": {"value": value, "unit": "shots/s", "cores": threads, "kind": "reference",
-                             "sample": desc},
+                             "sample": sample},
             "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-# ----------------------------------------------------------------- B200 arm
-def run_b200_arm(args):
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
+# ------------------------------------------------------ the survey's step
+def survey_step(eng, shots, stacks, world):
+    """One step of a survey on this rank: migrate its shots into its FP64 image
+    and illumination stacks (one contiguous float64 tensor, image first), then,
+    on N > 1, sum the stacks over all ranks in place (the path's one exchange)."""
+    n = stacks.numel() // 2
+    base = stacks.data_ptr()
+    eng.migrate_f64_into(shots, base, base + 8 * n)
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    from rtm_b200 import Engine, RTMParams, metrics
-    from rtm_b200.engine import ShotRecord
-
-    # The survey has SHOTS_PER_GPU * world shots; each rank takes a cost-balanced
-    # share (rtm_b200.shard: every rank computes the same assignment).
-    from rtm_b200 import shard
-    w_all = make_workload(args.shots * world, args.nt)
-    all_shots = w_all.shots
-    w = w_all
-    w.shots = shard.rank_shots(all_shots, rank, world, w.nx, w.nz, w.nb, w.nt)
-    model_traces(w, local)
-    nsh = len(w.shots)
-    n_img = w.nx * w.nz
-
-    p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=w.store_interval)
-    eng = Engine(args.mode, p, device=local, snap=args.snap, arithmetic=args.arith,
-                 max_shots_in_flight=args.max_in_flight, tile_cols=args.tile_cols)
-    eng.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-
-    # device-resident inputs and outputs for `value`
-    dev_tr = [torch.from_numpy(s.traces).to(f"cuda:{local}") for s in w.shots]
-    dev_shots = [ShotRecord(s.sx, s.sz, s.rx, s.rz, nt=s.nt, dt=s.dt, traces_ptr=t.data_ptr())
-                 for s, t in zip(w.shots, dev_tr)]
-    img = torch.zeros(n_img, dtype=torch.float32, device=f"cuda:{local}")
-    ill = torch.zeros_like(img)
-    stack = torch.zeros(2 * n_img, dtype=torch.float64, device=f"cuda:{local}")
-
-    def one_step(shots, img_ptr, ill_ptr):
-        eng.migrate_into(shots, img_ptr, ill_ptr)
-        if dist is not None:   # the one exchange of the path: sum the ranks' stacks
-            stack[:n_img].copy_(img)
-            stack[n_img:].copy_(ill)
-            shard.allreduce_stack(stack[:n_img], stack[n_img:])
-
-    for _ in range(args.warmup):
-        one_step(dev_shots, img.data_ptr(), ill.data_ptr())
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local) if rank == 0 else None
-    if sampler:
-        sampler.start()
-    eng.reset_times()
-    t_wall = time.perf_counter()
-    for _ in range(args.steps):
-        one_step(dev_shots, img.data_ptr(), ill.data_ptr())
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t_wall
-    tm = eng.times()
-    dev_time = tm["kernel"]
-    if dist is not None:
-        t = torch.tensor([dev_time, wall], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_time, wall = float(t[0]), float(t[1])
-        dist.barrier()
-    if sampler:
-        sampler.stop()
-    total_shots = nsh * world * args.steps
-    value = total_shots / dev_time
-    gcell = w.cell_updates() * world * args.steps / dev_time / 1e9
-    launches = tm["kernel_launches"]
-
-    # e2e through the C ABI with page-locked host traces and host outputs
-    pin_tr = [torch.from_numpy(s.traces).pin_memory() for s in w.shots]
-    host_shots = [ShotRecord(s.sx, s.sz, s.rx, s.rz, nt=s.nt, dt=s.dt, traces_ptr=t.data_ptr())
-                  for s, t in zip(w.shots, pin_tr)]
-    himg = torch.zeros(n_img, dtype=torch.float32).pin_memory()
-    hill = torch.zeros_like(himg).pin_memory()
-    one_step(host_shots, himg.data_ptr(), hill.data_ptr())   # warm
-    eng.reset_times()
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        one_step(host_shots, himg.data_ptr(), hill.data_ptr())
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_time = e0.elapsed_time(e1) * 1e-3
-    te = eng.times()
-    if dist is not None:
-        t = torch.tensor([e2e_time], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_time = float(t[0])
-    e2e = total_shots / e2e_time
-    h2d = te["h2d_bytes"] / args.steps
-    d2h = te["d2h_bytes"] / args.steps
-
-    # accuracy of the timed image against an FP64 run of the same scheme
-    rel64 = None
-    if not args.no_fp64_check:
-        img_h = himg.numpy().copy()
-        with Engine("batch", p, device=local, arithmetic="fp64") as e64:
-            e64.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-            ref64, _ = e64.migrate_f64(w.shots)
-        rel64 = metrics.compare_images(ref64, img_h)["l2_relative"]
-
-    l2_gbs = eng.memory_probe(48 << 20, 50)
-    tune = [r["pick"] for r in eng.autotune_report()]
-    eng.close()
-    if dist is not None:
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-
-    snap_b = {"f32": 4, "bf16": 2, "f16": 2}[args.snap]
-    algo_bytes = algorithmic_bytes_per_shot(w, snap_b) * nsh * args.steps
-    step_launches = max(1, launches)
-    achieved = algo_bytes / dev_time / 1e9          # this GPU's step-kernel bytes per device second
-    peak, peak_kind = read_peak()
-    traffic = read_traffic()
-    cpu = None
-    if not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        with tempfile.TemporaryDirectory() as td:
-            r = reference_sample(w_all if world == 1 else w, td, 300, threads)
-        if r:
-            upd_shot = 2.0 * w.nt * (w.nx + 2 * w.nb) * (w.nz + 2 * w.nb)
-            cpu = {"value": r[0] / upd_shot, "unit": "shots/s", "cores": threads, "kind": "reference",
-                   "sample": r[2]}
-    clocks = sampler.summary() if sampler else None
-    line = {
-        "metric": "shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dev_time / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": args.arith == "fma" and "f32-fma" or "f32",
-        "data": "synthetic (seeded model, GPU-modelled traces)",
-        "config": {"workload": f"config2: {w.nx}x{w.nz} @{w.dx:g} m, {nsh} shots/GPU, nt {w.nt}, "
-                               f"order {w.order}, store {w.store_interval}",
-                   "engine": args.mode, "max_shots_in_flight": args.max_in_flight, "tile_cols": args.tile_cols,
-                   "snapshots": args.snap, "arithmetic": args.arith, "accumulation": "compensated FP32 + FP64 stack",
-                   "l2": "inputs and snapshots larger than L2 (126 MB)", "autotuned_step_kernel": tune},
-        "gcell_updates_per_s": gcell,
-        "rel_l2_vs_fp64": rel64,
-        "gpu_launches": launches,
-        "wall_s_timed": wall,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic.get("bytes_per_launch") if traffic else None,
-                     "peak_source": peak_kind, "l2_copy_probe_gbs": l2_gbs,
-                     "algorithmic_bytes_per_step_launch": algo_bytes / step_launches},
-        "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "cpu_baseline": cpu,
-        "clocks": clocks,
-    }
-    print(json.dumps(line))
+        from rtm_b200 import shard
+        shard.allreduce_stacks_(stacks)
 
 
-# ------------------------------------------------------ other workloads
-def _timed_migrate(eng, shots, f64=False):
-    """One migration timed with the engine's CUDA events (device seconds)."""
-    eng.reset_times()
-    out = eng.migrate_f64(shots) if f64 else eng.migrate(shots)
-    return out, eng.times()
-
-
-def _model(w, device, shots=None):
+def _model_traces(w, device, shots=None):
     from rtm_b200 import Engine, RTMParams
     shots = shots if shots is not None else w.shots
     p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=1)
@@ -408,6 +297,240 @@ def _model(w, device, shots=None):
         s.traces = t
 
 
+def _image_metrics(ref, test):
+    a = np.asarray(ref, np.float64)
+    b = np.asarray(test, np.float64)
+    return {"rel_l2": float(np.linalg.norm(a - b) / max(np.linalg.norm(a), 1e-300)),
+            "max_abs": float(np.abs(a - b).max()),
+            "max_rel": float(np.abs(a - b).max() / max(np.abs(a).max(), 1e-300))}
+
+
+def _timed_migrate(eng, shots):
+    eng.reset_times()
+    eng.migrate(shots)
+    return eng.times()
+
+
+def run_survey(args, workload):
+    """The survey line (config3, the contract; or config2)."""
+    import datetime
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from rtm_b200 import Engine, RTMParams, shard, synth
+    from rtm_b200.engine import ShotRecord
+
+    per_gpu = args.shots or (256 if workload == "config3" else 64)
+    snap = args.snap or ("bf16" if workload == "config3" else "f32")
+    if workload == "config3":
+        w = synth.config3(nshots=per_gpu * world, order=args.order)
+    else:
+        w = synth.config2(nshots=per_gpu * world)
+    if args.nt:
+        w.nt = args.nt
+        for s in w.shots:
+            s.nt = args.nt
+    mine = shard.rank_shots(w.shots, rank, world, w.nx, w.nz, w.nb, w.nt)
+    _model_traces(w, local, mine)
+    n_img = w.nx * w.nz
+    p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=w.store_interval)
+    eng = Engine(args.mode, p, device=local, snap=snap, arithmetic=args.arith,
+                 max_shots_in_flight=args.max_in_flight, tile_cols=args.tile_cols)
+    eng.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+    dev = f"cuda:{local}"
+
+    # value: gathers resident in HBM, FP64 stacks on the device
+    dev_tr = [torch.from_numpy(s.traces).to(dev) for s in mine]
+    dev_shots = [ShotRecord(s.sx, s.sz, s.rx, s.rz, nt=s.nt, dt=s.dt, traces_ptr=t.data_ptr(),
+                            window_x0=s.window_x0, window_nx=s.window_nx) for s, t in zip(mine, dev_tr)]
+    stacks = torch.zeros(2 * n_img, dtype=torch.float64, device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step_device_time(shots):
+        """One step; returns (device seconds: engine stream + the exchange, launches)."""
+        eng.reset_times()
+        if world > 1:
+            eng.migrate_f64_into(shots, stacks.data_ptr(), stacks.data_ptr() + 8 * n_img)
+            ev0.record()
+            shard.allreduce_stacks_(stacks)
+            ev1.record()
+            torch.cuda.synchronize()
+            t = eng.times()
+            return t["kernel"] + ev0.elapsed_time(ev1) * 1e-3, t["kernel_launches"]
+        survey_step(eng, shots, stacks, world)
+        t = eng.times()
+        return t["kernel"], t["kernel_launches"]
+
+    for _ in range(args.warmup):
+        step_device_time(dev_shots)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    dev_time, launches = 0.0, 0
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        dt_s, nl = step_device_time(dev_shots)
+        dev_time += dt_s
+        launches += nl
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    if dist is not None:
+        t = torch.tensor([dev_time, wall], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_time, wall = float(t[0]), float(t[1])
+        dist.barrier()
+    if sampler:
+        sampler.stop()
+    total_shots = len(w.shots) * args.steps
+    value = total_shots / dev_time
+    gcell = cell_updates(w, w.shots) * args.steps / dev_time / 1e9
+    snap_b = {"f32": 4, "bf16": 2, "f16": 2}[snap]
+    algo_rank = algorithmic_bytes(w, mine, snap_b) * args.steps
+    tune = eng.autotune_report()
+
+    # e2e: page-locked host gathers in, host stacks out, through the C ABI
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    pin_tr = [torch.from_numpy(s.traces).pin_memory() for s in mine]
+    host_shots = [ShotRecord(s.sx, s.sz, s.rx, s.rz, nt=s.nt, dt=s.dt, traces_ptr=t.data_ptr(),
+                             window_x0=s.window_x0, window_nx=s.window_nx) for s, t in zip(mine, pin_tr)]
+    host_stacks = torch.zeros(2 * n_img, dtype=torch.float64).pin_memory()
+    survey_step(eng, host_shots[:1], stacks, 1)     # warm the host path (this rank alone)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    eng.reset_times()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        survey_step(eng, host_shots, stacks, world)
+        host_stacks.copy_(stacks, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_time = e0.elapsed_time(e1) * 1e-3
+    te = eng.times()
+    if dist is not None:
+        t = torch.tensor([e2e_time], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_time = float(t[0])
+    e2e = len(w.shots) * e2e_steps / e2e_time
+    h2d = te["h2d_bytes"] / e2e_steps
+    d2h = te["d2h_bytes"] / e2e_steps + 2 * n_img * 8
+
+    l2_gbs = eng.memory_probe(24 << 20, 200)   # 2 x 12 MB: resident in L2
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peak, peak_kind = read_peak()
+    traffic = read_traffic()
+    achieved = algo_rank / dev_time / 1e9
+    line = {
+        "metric": "shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_time / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model, GPU-modelled traces)",
+        "config": {"workload": (f"{workload}: {w.nx}x{w.nz} @{w.dx:g} m, {per_gpu} shots/GPU"
+                                + (", aperture windows 400-1150 columns (seed 3)" if workload == "config3" else "")
+                                + f", nt {w.nt}, order {w.order}, store {w.store_interval}"),
+                   "engine": args.mode, "snapshots": snap, "arithmetic": args.arith,
+                   "accumulation": "compensated FP32 per shot + FP64 stack",
+                   "max_shots_in_flight": args.max_in_flight or "engine choice", "tile_cols": args.tile_cols,
+                   "l2": "fields of the shots in flight, snapshots and gathers exceed L2 (126 MB)",
+                   "autotuned_step_kernel": [r["pick"] for r in tune]},
+        "gcell_updates_per_s": gcell,
+        "gpu_launches": launches,
+        "wall_s_timed": wall,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic.get("bytes_per_launch") if traffic else None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_step": algo_rank / args.steps, "l2_copy_gbs": l2_gbs},
+        "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "cpu_baseline": None,
+        "clocks": sampler.summary() if sampler else None,
+    }
+    if world == 1 and not args.no_extras:
+        line.update(survey_extras(args, w, p, snap, local, l2_gbs, value))
+    if world == 1 and not args.no_cpu_baseline and workload == "config3" and os.path.exists(REF_RTM):
+        threads = os.cpu_count() or 1
+        vm = _velocity_models()
+        with tempfile.TemporaryDirectory() as td:
+            sec, upd, wd = time_reference_shot(td, vm, w.vel, 0, w.order, threads, nt=w.nt)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "shots/s", "cores": threads, "kind": "reference",
+                                "sample": f"survey shot 0 whole (window {wd} columns, nt {w.nt}, "
+                                          f"{upd / 1e9:.2f} G cell updates), reference cpu-opt, wall time of the "
+                                          f"rtm process, random traces; {REF_BUILD}"}
+    print(json.dumps(line))
+
+
+def survey_extras(args, w, p, snap, dev, l2_gbs, batch_value):
+    """Single-GPU legs of the survey line: the plain FP32 engine on the same
+    shots (its ratio to the batched engine and its L2 roofline), the image
+    error of both against an FP64 run of the same scheme, and the order-12
+    survey."""
+    from rtm_b200 import Engine, RTMParams, synth
+    out = {}
+    plain_shots = w.shots[:args.plain_shots] if args.plain_shots else w.shots
+    with Engine("plain", p, device=dev) as e:
+        e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+        _timed_migrate(e, plain_shots[:2])
+        t = _timed_migrate(e, plain_shots)
+    plain = len(plain_shots) / t["kernel"]
+    l2b = stencil_bytes(w, plain_shots) / t["kernel"] / 1e9
+    out["plain_f32"] = {"shots_per_s": plain, "shots": len(plain_shots),
+                        "gcell_updates_per_s": t["cell_updates"] / t["kernel"] / 1e9,
+                        "roofline": {"bound": "l2", "achieved": l2b, "peak": l2_gbs, "unit": "GB/s",
+                                     "frac": l2b / l2_gbs, "what": "16 B per cell update of the two shots in flight "
+                                     "(L2-resident fields) per second, against the L2 copy probe"},
+                        "hbm_frac": algorithmic_bytes(w, plain_shots, 4) / t["kernel"] / 1e9 / read_peak()[0]}
+    out["speedup_vs_plain_f32"] = batch_value / plain
+    if not args.no_fp64_check:
+        chk = w.shots[:16]
+        with Engine("batch", p, device=dev, arithmetic="fp64") as e:
+            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+            ref64, _ = e.migrate_f64(chk)
+        acc = {}
+        for name, mode, sn in (("batch_" + snap, "batch", snap), ("plain_f32", "plain", "f32")):
+            with Engine(mode, p, device=dev, snap=sn) as e:
+                e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
+                img, _ = e.migrate(chk)
+            acc[name] = _image_metrics(ref64, img)
+        out["vs_fp64"] = {"subset": f"first {len(chk)} shots, FP64 GPU run of the same scheme", **acc}
+    if w.name.startswith("config3") and w.order == 8:
+        w12 = synth.config3(nshots=len(w.shots), order=12)
+        if args.nt:
+            w12.nt = args.nt
+            for s in w12.shots:
+                s.nt = args.nt
+        _model_traces(w12, dev)
+        p12 = RTMParams(nb=w12.nb, order=12, f0=w12.f0, store_interval=w12.store_interval)
+        with Engine("batch", p12, device=dev, snap=snap) as e:
+            e.setup(w12.vel, w12.nx, w12.nz, w12.dx, w12.dz, nt=w12.nt, dt=w12.dt)
+            _timed_migrate(e, w12.shots[:16])
+            t = _timed_migrate(e, w12.shots)
+        b12 = len(w12.shots) / t["kernel"]
+        sub = w12.shots[:64]
+        with Engine("plain", p12, device=dev) as e:
+            e.setup(w12.vel, w12.nx, w12.nz, w12.dx, w12.dz, nt=w12.nt, dt=w12.dt)
+            _timed_migrate(e, sub[:2])
+            tp = _timed_migrate(e, sub)
+        pl12 = len(sub) / tp["kernel"]
+        out["order12"] = {"batch_" + snap + "_shots_per_s": b12, "plain_f32_shots_per_s": pl12,
+                          "plain_shots": len(sub), "speedup_vs_plain_f32": b12 / pl12}
+    return out
+
+
+# ------------------------------------------------------ other workloads
 def run_config1(args):
     """The reference's CPU-runnable case (201 x 151, 3 flat layers, 4 shots,
     nt 1400, order 8, store 2, direct-wave mute 1500 m/s): the plain engine
@@ -419,7 +542,8 @@ def run_config1(args):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     w = synth.config1(dipping=False)
-    _model(w, dev)
+    _model_traces(w, dev)
+    raw = [s.traces.copy() for s in w.shots]
     t_pad = float(np.float32(1.0) / np.float32(w.f0))
     for sh in w.shots:
         mute_direct_wave(sh, w.mute_v, t_pad, t_pad)
@@ -429,26 +553,26 @@ def run_config1(args):
         with Engine(mode, p, device=dev) as e:
             e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
             _timed_migrate(e, w.shots)
-            (img, _), t = _timed_migrate(e, w.shots)
+            e.reset_times()
+            img, _ = e.migrate(w.shots)
+            t = e.times()
             res[name] = {"shots_per_s": len(w.shots) / t["kernel"], "gcell_updates_per_s":
                          t["cell_updates"] / t["kernel"] / 1e9, "seconds": t["kernel"]}
             imgs[name] = img
     cpu = {}
-    ref = os.path.join(ROOT, "oracle", "_ref", "rtm")
-    if os.path.exists(ref):
+    if os.path.exists(REF_RTM):
         with tempfile.TemporaryDirectory() as td:
             vel = os.path.join(td, "v.bin")
             rio.write_velocity_raw(vel, w.vel)
             rio.write_header_file(vel + ".hdr", rio.VelocityHeader(w.nx, w.nz, w.dx, w.dz, 0.0, 0.0, "zfast"))
             shp = os.path.join(td, "s.bin")
-            # the unmuted traces: the reference applies the mute itself
-            raw = synth.config1(dipping=False)
-            _model(raw, dev)
-            rio.write_shots_raw(shp, raw.shots)
+            for s, r in zip(w.shots, raw):   # the unmuted traces: the reference applies the mute itself
+                s.traces = r
+            rio.write_shots_raw(shp, w.shots)
             for eng, threads in (("cpu", 1), ("cpu-opt", os.cpu_count() or 1)):
                 out = os.path.join(td, f"{eng}.bin")
                 t0 = time.perf_counter()
-                subprocess.run([ref, "--engine", eng, "--velocity", vel, "--shots", shp, "--output", out,
+                subprocess.run([REF_RTM, "--engine", eng, "--velocity", vel, "--shots", shp, "--output", out,
                                 "--order", "8", "--nb", "60", "--f0", "12", "--store-interval", "2",
                                 "--mute-direct", "1500", "--quiet"], check=True, stdout=subprocess.DEVNULL,
                                env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
@@ -457,7 +581,7 @@ def run_config1(args):
                 cpu[eng] = {"shots_per_s": len(w.shots) / sec, "seconds_wall": sec, "threads": threads,
                             "plain_bit_identical": bool(np.array_equal(ref_img.view(np.uint32),
                                                                        imgs["plain"].view(np.uint32))),
-                            "batch_rel_l2": metrics.compare_images(ref_img, imgs["batch"])["l2_relative"]}
+                            "batch_vs_reference": metrics.compare_images(ref_img, imgs["batch"])}
     print(json.dumps({"workload": "config1", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
                       "value": res["plain"]["shots_per_s"], "b200": res, "reference_cpu": cpu,
                       "data": "synthetic (the reference's generator recipe, GPU-modelled traces)",
@@ -465,83 +589,30 @@ def run_config1(args):
                                  "mute": 1500}}))
 
 
-def run_config3(args):
-    """256 shots on uneven aperture windows (400-1150 columns of the
-    1150 x 400 model), orders 8 and 12: the batched engine (FP32 and BF16
-    snapshots, autotuned) against the plain one-shot-at-a-time engine."""
-    import torch
-    from rtm_b200 import Engine, RTMParams, metrics, synth
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    nshots = args.shots if args.shots != SHOTS_PER_GPU else 256
-    for order in (8, 12):
-        w = synth.config3(nshots=nshots, order=order)
-        _model(w, dev)
-        p = RTMParams(nb=w.nb, order=order, f0=w.f0, store_interval=w.store_interval)
-        res, times, images = {}, {}, {}
-        for name, mode, snap in (("batch_f32", "batch", "f32"), ("batch_bf16", "batch", "bf16")):
-            with Engine(mode, p, device=dev, snap=snap) as e:
-                e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-                _timed_migrate(e, w.shots[:16])                 # warm-up: autotune, graphs
-                (img, _), t = _timed_migrate(e, w.shots)
-                res[name] = len(w.shots) / t["kernel"]
-                times[name] = t
-                images[name] = img
-                tune = e.autotune_report()
-        sub = w.shots[:args.plain_shots]
-        with Engine("plain", p, device=dev) as e:
-            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-            _timed_migrate(e, sub[:2])
-            _, t = _timed_migrate(e, sub)
-            res["plain_f32"] = len(sub) / t["kernel"]
-            times["plain_f32"] = t
-        # accuracy on a 16-shot subset against an FP64 run of the same scheme
-        acc = {}
-        chk = w.shots[:16]
-        with Engine("batch", p, device=dev, arithmetic="fp64") as e:
-            e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-            ref64, _ = e.migrate_f64(chk)
-        for name, mode, snap in (("batch_f32", "batch", "f32"), ("batch_bf16", "batch", "bf16"),
-                                 ("plain_f32", "plain", "f32")):
-            with Engine(mode, p, device=dev, snap=snap) as e:
-                e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
-                img, _ = e.migrate(chk)
-            acc[name] = metrics.compare_images(ref64, img)["l2_relative"]
-        print(json.dumps({
-            "workload": f"config3-order{order}", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
-            "value": res["batch_bf16"], "batch_f32": res["batch_f32"], "batch_bf16": res["batch_bf16"],
-            "plain_f32": res["plain_f32"], "speedup_batch_bf16_vs_plain_f32": res["batch_bf16"] / res["plain_f32"],
-            "speedup_batch_f32_vs_plain_f32": res["batch_f32"] / res["plain_f32"],
-            "gcell_updates_per_s": {k: v["cell_updates"] / v["kernel"] / 1e9 for k, v in times.items()},
-            "rel_l2_vs_fp64": acc, "autotune": tune, "data": "synthetic (seeded model, GPU-modelled traces)",
-            "config": {"shots": len(w.shots), "plain_shots_timed": len(sub), "windows": "400-1150 columns, seed 3",
-                       "grid": f"{w.nx}x{w.nz} @{w.dx:g} m", "nt": w.nt, "order": order, "store": w.store_interval,
-                       "accuracy_subset": f"first {len(chk)} shots, FP64 GPU run of the same scheme"}}))
-        sys.stdout.flush()
-
-
 def run_config4(args):
     """4000 x 1500 cells at 5 m, order 12, 16 shots, nt 8000: BF16 and FP16
     snapshots with a power-of-two scale per column segment, Kahan FP32 per
     shot, FP64 stack."""
     import torch
-    from rtm_b200 import Engine, RTMParams, metrics, synth
+    from rtm_b200 import Engine, RTMParams, synth
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    nshots = args.shots if args.shots != SHOTS_PER_GPU else 16
-    w = synth.config4(nshots=nshots)
-    _model(w, dev)
+    w = synth.config4(nshots=args.shots or 16)
+    _model_traces(w, dev)
     p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=w.store_interval)
     res, gc, mem = {}, {}, {}
+    sampler = ClockSampler(dev)
+    sampler.start()
     for snap in ("bf16", "f16"):
         with Engine("batch", p, device=dev, snap=snap) as e:
             e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
             mem[snap] = e.snapshot_bytes
-            (_, _), t = _timed_migrate(e, w.shots)
+            t = _timed_migrate(e, w.shots)
             res[snap] = len(w.shots) / t["kernel"]
             gc[snap] = t["cell_updates"] / t["kernel"] / 1e9
-    # error against FP64: FP64 snapshots of the full time axis would need
-    # 195 GB per shot, so the comparison runs 2 shots on the first 2000 steps
+    sampler.stop()
+    # FP64 snapshots of the full time axis would need 195 GB per shot: the
+    # comparison runs 2 shots on the first 2000 steps
     nt_chk = 2000
     chk = w.shots[:2]
     acc = {}
@@ -552,11 +623,11 @@ def run_config4(args):
         with Engine("batch", p, device=dev, snap=snap) as e:
             e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=nt_chk, dt=w.dt)
             img, _ = e.migrate(chk)
-        acc[snap] = metrics.compare_images(ref64, img)["l2_relative"]
+        acc[snap] = _image_metrics(ref64, img)
     print(json.dumps({
         "workload": "config4", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
         "value": res["bf16"], "bf16": res["bf16"], "f16": res["f16"], "gcell_updates_per_s": gc,
-        "snapshot_bytes_per_shot": mem, "rel_l2_vs_fp64": acc,
+        "snapshot_bytes_per_shot": mem, "vs_fp64": acc, "clocks": sampler.summary(),
         "accuracy_run": f"{len(chk)} shots, nt truncated to {nt_chk} (FP64 snapshots of the full axis: 195 GB/shot)",
         "data": "synthetic (seeded model, GPU-modelled traces)",
         "config": {"grid": f"{w.nx}x{w.nz} @{w.dx:g} m", "shots": len(w.shots), "nt": w.nt, "order": w.order,
@@ -568,12 +639,12 @@ def run_config5(args):
     grids (201-2000 x 151-800), orders (8/12), time axes (1400-6000) and
     1-32 shots, admitted by snapshot memory, continuously batched."""
     import torch
-    from rtm_b200 import Engine, RTMParams, metrics, synth
+    from rtm_b200 import Engine, RTMParams, synth
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     reqs = synth.config5_stream(nreq=args.requests, rate_hz=1.0, seed=5)
     for r in reqs:
-        _model(r.work, dev)
+        _model_traces(r.work, dev)
     work = sum(r.work.cell_updates() for r in reqs)
     # arrival rate chosen so that the stream keeps the GPU about 90% busy at the
     # throughput of the batched engine (~150 G cell updates/s)
@@ -581,6 +652,8 @@ def run_config5(args):
     gaps = np.diff([0.0] + [r.arrival for r in reqs])
     scale = (0.9 * busy) / max(sum(gaps), 1e-9)
     arrivals = np.cumsum(gaps * scale)
+    sampler = ClockSampler(dev)
+    sampler.start()
     with Engine("serve", RTMParams(nb=60), device=dev, serve_max_nx=2000, serve_max_nz=800,
                 max_shots_in_flight=16) as e:
         t0 = e.clock()
@@ -607,6 +680,7 @@ def run_config5(args):
         lat = sorted(done[i][0]["finish_time"] - (t0 + arrivals[i]) for i in done)
         span = max(done[i][0]["finish_time"] for i in done) - (t0 + arrivals[0])
         shots = sum(len(r.work.shots) for r in reqs)
+    sampler.stop()
     # accuracy of the three smallest requests against FP64 runs of the same scheme
     acc = []
     for i in sorted(range(len(reqs)), key=lambda k: reqs[k].work.cell_updates())[:3]:
@@ -615,28 +689,28 @@ def run_config5(args):
                     arithmetic="fp64") as e64:
             e64.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
             ref64, _ = e64.migrate_f64(w.shots)
-        acc.append(metrics.compare_images(ref64, done[i][1])["l2_relative"])
-    q = lambda f: lat[min(len(lat) - 1, int(f * len(lat)))]
+        acc.append(_image_metrics(ref64, done[i][1]))
+    q = lambda f: lat[min(len(lat) - 1, int(f * len(lat)))]  # noqa: E731
     print(json.dumps({
         "workload": "config5", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
         "value": shots / span, "latency_s": {"p50": q(0.5), "p99": q(0.99), "max": lat[-1], "min": lat[0]},
         "gcell_updates_per_s": work / span / 1e9, "requests": len(reqs), "shots": shots,
         "offered_load": "arrivals scaled to keep the GPU ~90% busy at 150 G cell updates/s",
-        "rel_l2_vs_fp64_smallest3": acc, "data": "synthetic (seeded models, GPU-modelled traces)",
+        "vs_fp64_smallest3": acc, "data": "synthetic (seeded models, GPU-modelled traces)",
+        "clocks": sampler.summary(),
         "config": {"grids": "201-2000 x 151-800 @10 m", "orders": [8, 12], "nt": "1400-6000",
                    "shots_per_request": "1-32", "seed": 5}}))
 
 
-def main():
-    args = parse_args()
-    if args.impl != "reference" and args.workload != "config2":
-        {"config1": run_config1, "config3": run_config3, "config4": run_config4,
-         "config5": run_config5}[args.workload](args)
-        return
+def main(argv=None):
+    args = parse_args(argv)
     if args.impl == "reference":
         run_reference_arm(args)
-    else:
-        run_b200_arm(args)
+        return
+    if args.workload in ("config2", "config3"):
+        run_survey(args, args.workload)
+        return
+    {"config1": run_config1, "config4": run_config4, "config5": run_config5}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -185,6 +185,22 @@ RTM_B200_API int rtm_b200_migrate_f64(rtm_b200_engine* h, const rtm_b200_shot* s
 RTM_B200_API int rtm_b200_model_shots(rtm_b200_engine* h, const rtm_b200_shot* shots, int nshots,
                          float* traces_out);
 
+/* Post-processing of the stack the last rtm_b200_migrate / _migrate_f64 left on
+ * the device, computed on the device: the reference's
+ * illumination_compensation (I / (S + eps_relative * max S + 1e-30)) and
+ * laplacian_filter (second differences over dx^2 and dz^2 on the interior,
+ * zero on the outermost rows and columns), src/rtm/imaging.cpp:48-75, as its
+ * CLI applies them at src/main.cpp:211-223.  illum_out (nx*nz, may be NULL)
+ * receives the compensated image (the `_illum` output); filtered_out (may be
+ * NULL) receives the filtered image (the `_filtered` output), filtered after
+ * compensation when compensate_filtered is non-zero.  The plain engine works on
+ * its FP32 image with the reference's float operations (bit-identical to the
+ * reference's outputs); batch and serve work on the FP64 stack and round once at
+ * the end.  Buffers may be host or device memory of the engine's GPU.  ESTATE
+ * before any migration. */
+RTM_B200_API int rtm_b200_postprocess(rtm_b200_engine* h, float eps_relative, int compensate_filtered,
+                                      float* illum_out, float* filtered_out);
+
 /* Source propagation of one shot (reference forward_propagation,
  * include/rtm_engine.hpp:31-37).  snapshots (num_snapshots*nx*nz floats) and
  * recorded (nrec*nt) may each be NULL. */

@@ -134,6 +134,10 @@ public:
     void model_shot(ShotRecord& shot) override;
     // All shots modelled in one call (batched on the device).
     void model_shots(std::vector<ShotRecord>& shots);
+    // The `_illum` and `_filtered` outputs of the last migrate(), computed on
+    // the device (rtm_b200_postprocess); either pointer may be null.
+    void postprocess(float eps_relative, bool compensate_filtered, std::vector<float>* illum_out,
+                     std::vector<float>* filtered_out);
 
     int num_devices() const override { return 1; }
     std::string device_name() const override;

@@ -105,6 +105,13 @@ int rtm_b200_migrate_f64(rtm_b200_engine* h, const rtm_b200_shot* shots, int nsh
     return guarded(h, [&](rtmb::Engine& e) { return e.migrate(shots, nshots, nullptr, nullptr, image, illum); });
 }
 
+int rtm_b200_postprocess(rtm_b200_engine* h, float eps_relative, int compensate_filtered, float* illum_out,
+                         float* filtered_out) {
+    return guarded(h, [&](rtmb::Engine& e) {
+        return e.postprocess(eps_relative, compensate_filtered != 0, illum_out, filtered_out);
+    });
+}
+
 int rtm_b200_model_shots(rtm_b200_engine* h, const rtm_b200_shot* shots, int nshots, float* traces_out) {
     return guarded(h, [&](rtmb::Engine& e) { return e.model_shots(shots, nshots, traces_out); });
 }

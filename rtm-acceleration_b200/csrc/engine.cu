@@ -217,6 +217,7 @@ int Engine::setup(const float* vel, int nx, int nz, float dx, float dz, float ox
     RTMB_TRY(build_model(*m, vel, nx, nz, dx, dz, ox, oz, cfg_.order, nt, dt, cfg_.store_interval, cfg_.f0));
     model_ = std::move(m);
     keep_snap_ = false;
+    stack_ready_ = false;
     return RTM_B200_OK;
 }
 
@@ -1094,6 +1095,7 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
     RTMB_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     times.kernel += ms * 1e-3;
     const auto t_d2h = std::chrono::steady_clock::now();
+    stack_ready_ = true;
     RTMB_TRY(finalize_model_image(m, img, ill, img64, ill64));
     const auto t_end = std::chrono::steady_clock::now();
     times.d2h += std::chrono::duration<double>(t_end - t_d2h).count();
@@ -1248,6 +1250,49 @@ int Engine::memory_probe(size_t bytes, int iters, double* gbps) {
     RTMB_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     *gbps = 2.0 * (double)half * iters / (ms * 1e-3) / 1e9;
     launches_ += iters + 3;
+    return RTM_B200_OK;
+}
+
+// Post-processing of the finished stack on the device (reference
+// src/rtm/imaging.cpp:48-75 applied as at src/main.cpp:211-223).  Plain FP32:
+// the running FP32 image with the reference's float operations; otherwise the
+// FP64 stack (or the FP64 engine's image), rounded to float at the end.
+int Engine::postprocess(float eps_relative, bool compensate_filtered, float* illum_out, float* filtered_out) {
+    if (!model_ || !stack_ready_) return fail(RTM_B200_ESTATE, "postprocess before a migration");
+    RTMB_CUDA(cudaSetDevice(device_));
+    Model& m = *model_;
+    const GridDims& g = m.g;
+    const size_t n = (size_t)g.nx * g.nz;
+    const int row0 = g.nb - g.zs0;
+    const bool plain = cfg_.mode == RTM_B200_MODE_PLAIN;
+    const bool d64 = !plain || f64_;
+    const void* I = plain ? m.img.get() : m.img64.get();
+    const void* S = plain ? m.ill.get() : m.ill64.get();
+    const size_t es = d64 ? 8 : 4;
+    // scratch: max word, dense compensated (or raw) image, float outputs
+    const size_t o_dense = 256, o_out = o_dense + ((n * es + 255) & ~(size_t)255);
+    RTMB_CUDA(post_.reserve(o_out + 2 * n * 4));
+    char* base = post_.get<char>();
+    auto* smax = reinterpret_cast<unsigned long long*>(base);
+    void* dense = base + o_dense;
+    float* out_c = reinterpret_cast<float*>(base + o_out);
+    float* out_f = out_c + n;
+    RTMB_CUDA(cudaMemsetAsync(smax, 0, sizeof(unsigned long long), stream_));
+    RTMB_CUDA(launch_stack_max(S, d64, g.nx, g.nz, g.lds, row0, smax, stream_));
+    if (illum_out || (filtered_out && compensate_filtered))
+        RTMB_CUDA(launch_compensate(I, S, d64, g.nx, g.nz, g.lds, row0, eps_relative, smax, dense, out_c, stream_));
+    if (filtered_out) {
+        if (!compensate_filtered) RTMB_CUDA(launch_extract_dense(I, d64, g.nx, g.nz, g.lds, row0, dense, stream_));
+        // the reference's weights are float: 1.0f / (dx * dx)
+        const float wxf = 1.0f / (m.dx * m.dx), wzf = 1.0f / (m.dz * m.dz);
+        const double wx = d64 ? 1.0 / ((double)m.dx * m.dx) : (double)wxf;
+        const double wz = d64 ? 1.0 / ((double)m.dz * m.dz) : (double)wzf;
+        RTMB_CUDA(launch_laplacian(dense, d64, g.nx, g.nz, wx, wz, out_f, stream_));
+    }
+    launches_ += 3;
+    if (illum_out) RTMB_CUDA(cudaMemcpyAsync(illum_out, out_c, n * 4, cudaMemcpyDefault, stream_));
+    if (filtered_out) RTMB_CUDA(cudaMemcpyAsync(filtered_out, out_f, n * 4, cudaMemcpyDefault, stream_));
+    RTMB_CUDA(cudaStreamSynchronize(stream_));
     return RTM_B200_OK;
 }
 

@@ -105,6 +105,7 @@ public:
     int forward(const rtm_b200_shot* shot, float* snaps, float* rec);
     int backward(const rtm_b200_shot* shot, const float* snaps, float* img, float* ill);
     int imaging(const float* fwd, const float* bwd, float* img, float* ill);
+    int postprocess(float eps_relative, bool compensate_filtered, float* illum_out, float* filtered_out);
 
     int submit(const rtm_b200_request* req, long long* ticket);
     int serve_step(int max_steps, int* pending);
@@ -180,6 +181,8 @@ private:
     std::chrono::steady_clock::time_point t0_;
 
     std::unique_ptr<Model> model_;           // the setup() model
+    bool stack_ready_ = false;               // model_'s stack holds a finished migration
+    DevMem post_;                            // post-processing scratch
 
     // field pool: T[nslots][3][nxe_cap][ldz_cap]
     DevMem pool_;

@@ -104,6 +104,16 @@ void B200RTM::migrate(const std::vector<ShotRecord>& shots, std::vector<float>& 
     copy_times();
 }
 
+void B200RTM::postprocess(float eps_relative, bool compensate_filtered, std::vector<float>* illum_out,
+                          std::vector<float>* filtered_out) {
+    if (!h_) throw std::runtime_error("postprocess before setup");
+    if (illum_out) illum_out->assign(g_.n_interior(), 0.0f);
+    if (filtered_out) filtered_out->assign(g_.n_interior(), 0.0f);
+    check(rtm_b200_postprocess(h_, eps_relative, compensate_filtered ? 1 : 0, illum_out ? illum_out->data() : nullptr,
+                               filtered_out ? filtered_out->data() : nullptr),
+          "postprocess");
+}
+
 void B200RTM::forward_propagation(const ShotRecord& shot, std::vector<float>* snapshots,
                                   std::vector<float>* recorded) {
     if (!h_) throw std::runtime_error("forward_propagation before setup");

@@ -381,6 +381,147 @@ cudaError_t launch_copy_probe(const float4* src, float4* dst, size_t n, cudaStre
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------ post-processing
+template <typename T>
+__global__ void stack_max_kernel(const T* __restrict__ S, int nx, int nz, int lds, int row0,
+                                 unsigned long long* smax_bits) {
+    __shared__ double part[32];
+    double m = 0.0;   // the reference starts its running max at 0
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        const double v = (double)S[(size_t)ix * lds + row0 + iz];
+        m = v > m ? v : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x + 31) / 32 ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, m, o);
+            m = t > m ? t : m;
+        }
+        if (threadIdx.x == 0) atomicMax(smax_bits, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void compensate_f32_kernel(const float* __restrict__ I, const float* __restrict__ S, int nx, int nz,
+                                      int lds, int row0, float eps_rel, const unsigned long long* smax_bits,
+                                      float* __restrict__ dense, float* __restrict__ out) {
+    // eps = eps_rel * smax + 1e-30 in float, then I / (S + eps) (imaging.cpp:53-57)
+    const float smax = (float)__longlong_as_double((long long)*smax_bits);
+    const float eps = __fadd_rn(__fmul_rn(eps_rel, smax), 1e-30f);
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        const size_t k = (size_t)ix * lds + row0 + iz;
+        const float v = __fdiv_rn(I[k], __fadd_rn(S[k], eps));
+        if (dense) dense[i] = v;
+        if (out) out[i] = v;
+    }
+}
+
+__global__ void compensate_f64_kernel(const double* __restrict__ I, const double* __restrict__ S, int nx, int nz,
+                                      int lds, int row0, double eps_rel, const unsigned long long* smax_bits,
+                                      double* __restrict__ dense, float* __restrict__ out) {
+    const double eps = eps_rel * __longlong_as_double((long long)*smax_bits) + 1e-30;
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        const size_t k = (size_t)ix * lds + row0 + iz;
+        const double v = I[k] / (S[k] + eps);
+        if (dense) dense[i] = v;
+        if (out) out[i] = (float)v;
+    }
+}
+
+template <typename T>
+__global__ void extract_dense_kernel(const T* __restrict__ I, int nx, int nz, int lds, int row0,
+                                     T* __restrict__ dense) {
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        dense[i] = I[(size_t)ix * lds + row0 + iz];
+    }
+}
+
+__global__ void laplacian_f32_kernel(const float* __restrict__ in, int nx, int nz, float wx, float wz,
+                                     float* __restrict__ out) {
+    // wx ((a - 2 b) + c) + wz ((d - 2 b) + e), each operation rounded on its
+    // own like the reference's -O2 build (imaging.cpp:65-75)
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        float v = 0.0f;
+        if (ix >= 1 && ix + 1 < nx && iz >= 1 && iz + 1 < nz) {
+            const float b2 = __fmul_rn(2.0f, in[i]);
+            const float sx = __fadd_rn(__fsub_rn(in[i + nz], b2), in[i - nz]);
+            const float sz = __fadd_rn(__fsub_rn(in[i + 1], b2), in[i - 1]);
+            v = __fadd_rn(__fmul_rn(wx, sx), __fmul_rn(wz, sz));
+        }
+        out[i] = v;
+    }
+}
+
+__global__ void laplacian_f64_kernel(const double* __restrict__ in, int nx, int nz, double wx, double wz,
+                                     float* __restrict__ out) {
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        double v = 0.0;
+        if (ix >= 1 && ix + 1 < nx && iz >= 1 && iz + 1 < nz)
+            v = wx * (in[i + nz] - 2.0 * in[i] + in[i - nz]) + wz * (in[i + 1] - 2.0 * in[i] + in[i - 1]);
+        out[i] = (float)v;
+    }
+}
+
+cudaError_t launch_stack_max(const void* S, bool f64, int nx, int nz, int lds, int row0,
+                             unsigned long long* smax_bits, cudaStream_t s) {
+    const int g = grid_for((size_t)nx * nz);
+    if (f64)
+        stack_max_kernel<double><<<g, 256, 0, s>>>((const double*)S, nx, nz, lds, row0, smax_bits);
+    else
+        stack_max_kernel<float><<<g, 256, 0, s>>>((const float*)S, nx, nz, lds, row0, smax_bits);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compensate(const void* I, const void* S, bool f64, int nx, int nz, int lds, int row0,
+                              float eps_rel, const unsigned long long* smax_bits, void* dense, float* out,
+                              cudaStream_t s) {
+    const int g = grid_for((size_t)nx * nz);
+    if (f64)
+        compensate_f64_kernel<<<g, 256, 0, s>>>((const double*)I, (const double*)S, nx, nz, lds, row0,
+                                                (double)eps_rel, smax_bits, (double*)dense, out);
+    else
+        compensate_f32_kernel<<<g, 256, 0, s>>>((const float*)I, (const float*)S, nx, nz, lds, row0, eps_rel,
+                                                smax_bits, (float*)dense, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_extract_dense(const void* I, bool f64, int nx, int nz, int lds, int row0, void* dense,
+                                 cudaStream_t s) {
+    const int g = grid_for((size_t)nx * nz);
+    if (f64)
+        extract_dense_kernel<double><<<g, 256, 0, s>>>((const double*)I, nx, nz, lds, row0, (double*)dense);
+    else
+        extract_dense_kernel<float><<<g, 256, 0, s>>>((const float*)I, nx, nz, lds, row0, (float*)dense);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_laplacian(const void* in, bool f64, int nx, int nz, double wx, double wz, float* out,
+                             cudaStream_t s) {
+    const int g = grid_for((size_t)nx * nz);
+    if (f64)
+        laplacian_f64_kernel<<<g, 256, 0, s>>>((const double*)in, nx, nz, wx, wz, out);
+    else
+        laplacian_f32_kernel<<<g, 256, 0, s>>>((const float*)in, nx, nz, (float)wx, (float)wz, out);
+    return cudaGetLastError();
+}
+
 __global__ void widen_kernel(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         dst[i] = (double)src[i];

@@ -104,6 +104,28 @@ cudaError_t launch_imaging_dense(const float* fwd, const float* bwd_ext, float* 
 // dst[i] = src[i] over n float4 elements (bandwidth probe).
 cudaError_t launch_copy_probe(const float4* src, float4* dst, size_t n, cudaStream_t s);
 
+// Post-processing of a finished stack (reference illumination_compensation and
+// laplacian_filter, src/rtm/imaging.cpp:48-75).  S and I are in the padded
+// stack layout (nx columns of lds rows, interior rows from row0).
+// smax_bits <- bits of max(0, max S) as a double (S >= 0, so the bit patterns
+// order like the values); clear it to 0 first.
+cudaError_t launch_stack_max(const void* S, bool f64, int nx, int nz, int lds, int row0,
+                             unsigned long long* smax_bits, cudaStream_t s);
+// dense[ix*nz+iz] = I / (S + eps), eps = eps_rel * smax + 1e-30, in the
+// stack's precision (FP32: the reference's float operations bit for bit).
+// dense is T (float or double); out (may be null) receives it as float.
+cudaError_t launch_compensate(const void* I, const void* S, bool f64, int nx, int nz, int lds, int row0,
+                              float eps_rel, const unsigned long long* smax_bits, void* dense, float* out,
+                              cudaStream_t s);
+// dense (nx*nz, T) -> raw image copy (no compensation), for the filter input.
+cudaError_t launch_extract_dense(const void* I, bool f64, int nx, int nz, int lds, int row0, void* dense,
+                                 cudaStream_t s);
+// out[i] = wx (in[i+nz] - 2 in[i] + in[i-nz]) + wz (in[i+1] - 2 in[i] + in[i-1])
+// on the interior, 0 on the outermost rows and columns; FP32 in the reference's
+// operation order, or FP64 for a double input.
+cudaError_t launch_laplacian(const void* in, bool f64, int nx, int nz, double wx, double wz, float* out,
+                             cudaStream_t s);
+
 // float -> double widening of a dense array.
 cudaError_t launch_widen(const float* src, double* dst, size_t n, cudaStream_t s);
 

@@ -177,16 +177,27 @@ int main(int argc, char** argv) try {
     const auto dot = out_path.find_last_of('.');
     const std::string stem = dot == std::string::npos ? out_path : out_path.substr(0, dot);
     if (want_map) io::write_raw_floats(stem + "_illummap.bin", illum);
-    if (want_illum) {
-        std::vector<float> t = image;
-        illumination_compensation(t, illum, 1e-4f);
-        io::write_raw_floats(stem + "_illum.bin", t);
-    }
-    if (filter == "laplacian") {
-        std::vector<float> t = image;
-        if (want_illum) illumination_compensation(t, illum, 1e-4f);
-        laplacian_filter(t, g);
-        io::write_raw_floats(stem + "_filtered.bin", t);
+    // _illum and _filtered (reference src/main.cpp:211-223): computed on the
+    // device from the stack the migration left there for the B200 engines, on
+    // the host otherwise.
+    auto* b200 = dynamic_cast<B200RTM*>(engine.get());
+    if (b200 && (want_illum || filter == "laplacian")) {
+        std::vector<float> ti, tf;
+        b200->postprocess(1e-4f, want_illum, want_illum ? &ti : nullptr, filter == "laplacian" ? &tf : nullptr);
+        if (want_illum) io::write_raw_floats(stem + "_illum.bin", ti);
+        if (filter == "laplacian") io::write_raw_floats(stem + "_filtered.bin", tf);
+    } else {
+        if (want_illum) {
+            std::vector<float> t = image;
+            illumination_compensation(t, illum, 1e-4f);
+            io::write_raw_floats(stem + "_illum.bin", t);
+        }
+        if (filter == "laplacian") {
+            std::vector<float> t = image;
+            if (want_illum) illumination_compensation(t, illum, 1e-4f);
+            laplacian_filter(t, g);
+            io::write_raw_floats(stem + "_filtered.bin", t);
+        }
     }
 
     // Report: the reference's cell-update convention (2 nt N_ext per shot).

@@ -109,6 +109,7 @@ def load():
         "rtm_b200_drain": (C.c_int, [E]),
         "rtm_b200_clock": (C.c_double, [E]),
         "rtm_b200_memory_probe": (C.c_int, [E, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
+        "rtm_b200_postprocess": (C.c_int, [E, C.c_float, C.c_int, vp, vp]),
         "rtm_b200_model_shot_static": (C.c_int, [C.POINTER(StaticProblem), C.POINTER(Shot), vp, C.c_char_p,
                                                  C.c_size_t]),
     }

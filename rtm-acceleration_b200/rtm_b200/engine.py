@@ -174,6 +174,15 @@ class Engine:
         self._check(self.lib.rtm_b200_migrate(self.h, arr, len(shots), C.cast(C.c_void_p(img_ptr), fp),
                                               C.cast(C.c_void_p(ill_ptr), fp)), "migrate")
 
+    def migrate_f64_into(self, shots: Sequence[ShotRecord], img_ptr: int, ill_ptr: int):
+        """migrate_f64() writing the nx*nz FP64 stacks to raw addresses (device
+        memory of the engine's GPU, or host memory)."""
+        keep: list = []
+        arr = shots_to_c(shots, keep)
+        dp = C.POINTER(C.c_double)
+        self._check(self.lib.rtm_b200_migrate_f64(self.h, arr, len(shots), C.cast(C.c_void_p(img_ptr), dp),
+                                                  C.cast(C.c_void_p(ill_ptr), dp)), "migrate_f64")
+
     def migrate_f64(self, shots: Sequence[ShotRecord]) -> Tuple[np.ndarray, np.ndarray]:
         keep: list = []
         arr = shots_to_c(shots, keep)
@@ -181,6 +190,16 @@ class Engine:
         ill = np.zeros_like(img)
         self._check(self.lib.rtm_b200_migrate_f64(self.h, arr, len(shots), _dp(img), _dp(ill)), "migrate_f64")
         return img, ill
+
+    def postprocess(self, eps_relative: float = 1e-4, compensate_filtered: bool = True):
+        """(illumination-compensated image, Laplacian-filtered image) of the last
+        migration, computed on the device (reference imaging.cpp:48-75 as its
+        CLI applies them)."""
+        ic = np.zeros(self.nx * self.nz, np.float32)
+        fl = np.zeros_like(ic)
+        self._check(self.lib.rtm_b200_postprocess(self.h, float(eps_relative), 1 if compensate_filtered else 0,
+                                                  ic.ctypes.data, fl.ctypes.data), "postprocess")
+        return ic, fl
 
     def model_shots(self, shots: Sequence[ShotRecord]) -> List[np.ndarray]:
         keep: list = []

@@ -37,19 +37,30 @@ def rank_shots(shots, rank: int, world: int, nx: int, nz: int, nb: int, nt: int)
     return [shots[i] for i in assign_shots(costs, world)[rank]]
 
 
-def allreduce_stack(image: np.ndarray | None, illum: np.ndarray | None, group=None, device=None):
-    """Sum the FP64 image and illumination stacks of every rank (one all-reduce
-    of 2*nx*nz doubles).  Accepts numpy arrays or torch tensors; returns the
-    summed pair as the same kind."""
+def allreduce_stacks_(stacks, group=None):
+    """Sum every rank's FP64 stacks in place: ``stacks`` is one contiguous
+    float64 tensor holding the image stack followed by the illumination stack
+    (2*nx*nz doubles, on the rank's GPU for NCCL or on the host for gloo).  One
+    all-reduce, the only exchange of the multi-GPU path."""
     import torch
     import torch.distributed as dist
+    if stacks.dtype != torch.float64 or not stacks.is_contiguous():
+        raise ValueError("stacks must be one contiguous float64 tensor")
+    dist.all_reduce(stacks, op=dist.ReduceOp.SUM, group=group)
+    return stacks
+
+
+def allreduce_stack(image, illum, group=None, device=None):
+    """Sum the FP64 image and illumination stacks of every rank; numpy arrays
+    in, numpy arrays out (host copies), or torch tensors in and out."""
+    import torch
     as_numpy = isinstance(image, np.ndarray)
     a = torch.as_tensor(image, dtype=torch.float64).reshape(-1)
     b = torch.as_tensor(illum, dtype=torch.float64).reshape(-1)
     buf = torch.cat([a, b])
     if device is not None:
         buf = buf.to(device)
-    dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+    allreduce_stacks_(buf, group)
     n = a.numel()
     ri, rs = buf[:n], buf[n:]
     if as_numpy:

@@ -249,3 +249,42 @@ def test_parameter_validation_errors():
             e.migrate([short])
         img, _ = e.migrate(shots)            # engine still usable after errors
         assert np.isfinite(img).all()
+
+
+def _post_reference_f32(img, ill, nx, nz, dx, dz, eps_rel=np.float32(1e-4)):
+    """The reference's float post-processing (imaging.cpp:48-75, main.cpp:211-223)
+    restated with one numpy float32 operation per C operation."""
+    f = np.float32
+    smax = max(f(0), ill.max())
+    eps = f(eps_rel * smax) + f(1e-30)
+    comp = (img / (ill + eps)).astype(np.float32)
+    a = comp.reshape(nx, nz)
+    out = np.zeros_like(a)
+    wx, wz = f(1) / f(f(dx) * f(dx)), f(1) / f(f(dz) * f(dz))
+    b2 = f(2) * a[1:-1, 1:-1]
+    sx = (a[2:, 1:-1] - b2) + a[:-2, 1:-1]
+    sz = (a[1:-1, 2:] - b2) + a[1:-1, :-2]
+    out[1:-1, 1:-1] = wx * sx + wz * sz
+    return comp, out.ravel()
+
+
+def test_device_postprocess_plain_bit_exact_and_batch_vs_fp64():
+    """`_illum` and `_filtered` computed on the device: bit-identical to the
+    reference's float formulas from the plain engine's FP32 image, and within
+    1e-5 of the FP64 formulas from the batch engine's FP64 stack."""
+    p, v, shots = random_problem(seed=44, order=8, nx=72, nz=48, nb=10, nt=160, si=2)
+    with make_engine("plain", p, v) as e:
+        img, ill = e.migrate(shots)
+        comp, filt = e.postprocess(1e-4, True)
+    rc, rf = _post_reference_f32(img, ill, p.nx, p.nz, p.dx, p.dz)
+    assert bits_equal(comp, rc) and bits_equal(filt, rf)
+    with make_engine("batch", p, v) as e:
+        i64, s64 = e.migrate_f64(shots)
+        comp_b, filt_b = e.postprocess(1e-4, True)
+    c64 = i64 / (s64 + (1e-4 * max(0.0, s64.max()) + 1e-30))
+    a = c64.reshape(p.nx, p.nz)
+    f64 = np.zeros_like(a)
+    f64[1:-1, 1:-1] = ((a[2:, 1:-1] - 2 * a[1:-1, 1:-1] + a[:-2, 1:-1]) / p.dx ** 2 +
+                       (a[1:-1, 2:] - 2 * a[1:-1, 1:-1] + a[1:-1, :-2]) / p.dz ** 2)
+    assert rel_l2(c64, comp_b) < 1e-6 and rel_l2(f64.ravel(), filt_b) < 1e-5
+    assert rel_l2(rc, comp_b) < 1e-4
