@@ -53,6 +53,13 @@ extern "C" {
 #define RTM_B200_SNAP_F32  0
 #define RTM_B200_SNAP_BF16 1   /* power-of-two scale per 128-cell segment     */
 #define RTM_B200_SNAP_F16  2
+#define RTM_B200_SNAP_RECON 3  /* no snapshots (batch/serve, FP32): the forward
+                                  pass stores the band of order/2 cells around
+                                  the interior at every step, the backward pass
+                                  rebuilds the source field in reverse time
+                                  inside the interior (snapshot-free source
+                                  reconstruction); about 2*order*(nx+nz)*nt*4
+                                  bytes per shot instead of nt/si*nx*nz*s */
 
 /* ---- arithmetic --------------------------------------------------------- */
 #define RTM_B200_ARITH_IEEE 0  /* FP32, unfused, reference operation order:
@@ -272,6 +279,12 @@ RTM_B200_API void rtm_b200_mute_direct_wave(const rtm_b200_shot* shot, float* tr
  * and reports read+write bytes per second.  A buffer well under the 126 MB L2
  * measures L2 bandwidth, one of several GB measures HBM. */
 RTM_B200_API int rtm_b200_memory_probe(rtm_b200_engine* h, size_t bytes, int iters, double* gbps);
+
+/* L2 read bandwidth on the engine's GPU: a buffer of `bytes` (small enough to
+ * stay in the 126 MB L2, e.g. 24 MB) read `reps` times per launch through L2,
+ * bypassing L1.  The roofline peak for work whose fields stay in L2.  The
+ * reference has no L2 probe; its rtm_bandwidth_probe measures DRAM. */
+RTM_B200_API int rtm_b200_l2_probe(rtm_b200_engine* h, size_t bytes, int reps, double* gbps);
 
 /* ---- modelling without any GPU allocation ------------------------------- */
 

@@ -181,6 +181,20 @@ int rtm_b200_autotune_report(const rtm_b200_engine* h, char* buf, size_t len) {
         for (size_t k = 0; k < r.cands.size(); ++k) js += (k ? ", " : "") + choice(r.cands[k]);
         js += "], \"pick\": " + choice(r.pick) + "}";
     }
+    for (const auto& t : h->e->inflight_log_) {
+        js += js.size() > 1 ? ", {" : "{";
+        js += "\"kind\": \"shots_in_flight\", \"key\": [";
+        for (size_t k = 0; k < t.key.size(); ++k) js += (k ? ", " : "") + std::to_string(t.key[k]);
+        js += "], \"candidates\": [";
+        for (size_t k = 0; k < t.cands.size(); ++k) js += (k ? ", " : "") + std::to_string(t.cands[k]);
+        js += "], \"shots_per_s\": [";
+        for (size_t k = 0; k < t.shots_per_s.size(); ++k) {
+            char v[32];
+            std::snprintf(v, sizeof v, "%s%.3f", k ? ", " : "", t.shots_per_s[k]);
+            js += v;
+        }
+        js += "], \"pick\": " + std::to_string(t.pick) + "}";
+    }
     js += "]";
     copy_str(js, buf, len);
     return js.size() < len ? RTM_B200_OK : RTM_B200_EINVAL;
@@ -216,6 +230,10 @@ double rtm_b200_clock(const rtm_b200_engine* h) { return (h && h->e) ? h->e->clo
 
 int rtm_b200_memory_probe(rtm_b200_engine* h, size_t bytes, int iters, double* gbps) {
     return guarded(h, [&](rtmb::Engine& e) { return e.memory_probe(bytes, iters, gbps); });
+}
+
+int rtm_b200_l2_probe(rtm_b200_engine* h, size_t bytes, int reps, double* gbps) {
+    return guarded(h, [&](rtmb::Engine& e) { return e.l2_probe(bytes, reps, gbps); });
 }
 
 }  // extern "C"

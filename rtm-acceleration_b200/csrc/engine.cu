@@ -102,10 +102,15 @@ int Engine::init() {
         return fail(RTM_B200_EINVAL, "unknown engine mode");
     if (cfg_.arithmetic < RTM_B200_ARITH_IEEE || cfg_.arithmetic > RTM_B200_ARITH_FP64)
         return fail(RTM_B200_EINVAL, "unknown arithmetic");
-    if (cfg_.snap_precision < RTM_B200_SNAP_F32 || cfg_.snap_precision > RTM_B200_SNAP_F16)
+    if (cfg_.snap_precision < RTM_B200_SNAP_F32 || cfg_.snap_precision > RTM_B200_SNAP_RECON)
         return fail(RTM_B200_EINVAL, "unknown snapshot precision");
     if (f64_ && cfg_.snap_precision != RTM_B200_SNAP_F32)
         return fail(RTM_B200_EINVAL, "the FP64 engine stores FP64 snapshots (snap_precision must be F32)");
+    if (cfg_.snap_precision == RTM_B200_SNAP_RECON && cfg_.mode == RTM_B200_MODE_PLAIN)
+        return fail(RTM_B200_EINVAL, "source reconstruction needs the batch or serve engine (the plain engine keeps "
+                                     "the reference's snapshots, bit for bit)");
+    recon_ = cfg_.snap_precision == RTM_B200_SNAP_RECON;
+    nbuf_ = recon_ ? kReconBuffers : kFieldBuffers;
     if (cfg_.tile_cols != 0 && cfg_.tile_cols != 16 && cfg_.tile_cols != 32)
         return fail(RTM_B200_EINVAL, "tile_cols must be 0, 16 or 32");
     int n = 0;
@@ -224,6 +229,7 @@ int Engine::setup(const float* vel, int nx, int nz, float dx, float dz, float ox
 int Engine::snap_type() const {
     if (f64_) return kSnapF64;
     switch (cfg_.snap_precision) {
+        case RTM_B200_SNAP_RECON: return kSnapNone;
         case RTM_B200_SNAP_BF16: return kSnapBF16;
         case RTM_B200_SNAP_F16: return kSnapF16;
         default: return kSnapF32;
@@ -232,6 +238,8 @@ int Engine::snap_type() const {
 
 size_t Engine::snap_alloc_bytes(const Model& m, const GridDims& gs) const {
     const int st = snap_type();
+    if (st == kSnapNone)   // boundary strips of levels 1..nt-1
+        return round256((size_t)std::max(m.nt - 1, 1) * strip_cells(gs.nx, gs.nz, m.half) * 4);
     const size_t es = st == kSnapF64 ? 8 : (st == kSnapF32 ? 4 : 2);
     size_t b = round256((size_t)m.nsnap * gs.nx * gs.lds * es);
     if (st == kSnapBF16 || st == kSnapF16) b += round256((size_t)m.nsnap * gs.nx * gs.ntz);
@@ -283,7 +291,7 @@ StepVariant Engine::variant(int half) const {
     v.tile_x = tile_x_;
     v.warps = f64_ ? 8 : warps_;
     v.exact = exact();
-    v.kind = f64_ ? kStepRing : kind_;
+    v.kind = (f64_ || recon_) ? kStepRing : kind_;   // the march kernel has no reconstruction
     v.march_m = march_m_;
     v.nstage = step_default_stages(v);
     if (stage_override_ > 0) {
@@ -296,7 +304,7 @@ StepVariant Engine::variant(int half) const {
 
 int Engine::encode_map(int half, bool with_halo, CUtensorMap* out) {
     const StepVariant v = variant(half);
-    const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)nslots_ * kFieldBuffers};
+    const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)nslots_ * nbuf_};
     const cuuint64_t strides[2] = {(cuuint64_t)ldz_cap_ * elem(), (cuuint64_t)ldz_cap_ * nxe_cap_ * elem()};
     const cuuint32_t box[3] = {(cuuint32_t)(with_halo ? step_box_z(v) : kTileZ),
                                (cuuint32_t)(with_halo ? step_box_x(v) : step_tile_x(v)), 1};
@@ -319,7 +327,7 @@ int Engine::ensure_pool(int nslots, int nxe_cap, int ldz_cap) {
     nslots_ = std::max(nslots, nslots_);
     nxe_cap_ = std::max(nxe_cap, nxe_cap_);
     ldz_cap_ = ldz_cap;
-    const size_t bytes = (size_t)nslots_ * kFieldBuffers * nxe_cap_ * ldz_cap_ * elem();
+    const size_t bytes = (size_t)nslots_ * nbuf_ * nxe_cap_ * ldz_cap_ * elem();
     cudaError_t e = pool_.alloc(bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -458,6 +466,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     d.nxe = gs.nxe; d.nze = gs.nze; d.nx = gs.nx; d.nz = gs.nz; d.nb = gs.nb;
     d.model_x0 = sh.x0; d.win_nx = gs.nx;
     d.zs0 = gs.zs0; d.lds = gs.lds; d.ntz = gs.ntz;
+    d.bsize = recon_ ? strip_cells(gs.nx, gs.nz, m->half) : 0;
     d.nt = m->nt; d.si = m->si; d.nsnap = m->nsnap;
     job.first_phase_step = backward_only == 1 ? m->nt : 0;
     job.g0 = g_ - job.first_phase_step;
@@ -495,6 +504,8 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     } else if (backward_only == 2) {
         d.flags = kFlagSnapshots | (rec_host ? kFlagRecord : 0);   // forward() of the method API
         d.total_steps = job.total = m->nt;
+    } else if (recon_) {
+        d.flags = kFlagRecon | kFlagImage;
     } else {
         d.flags = (backward_only ? 0 : kFlagSnapshots) | kFlagImage;
     }
@@ -550,7 +561,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                               stream_));
     // The slot's (v dt)^2 on the shot's extended grid (third field buffer).
     {
-        char* vbuf = pool_.get<char>() + ((size_t)s * kFieldBuffers + 2) * nxe_cap_ * ldz_cap_ * elem();
+        char* vbuf = pool_.get<char>() + ((size_t)s * nbuf_ + 2) * nxe_cap_ * ldz_cap_ * elem();
         RTMB_CUDA(launch_slot_vdt2(vbuf, f64_, ldz_cap_, gs.nxe, m->vdt2.get<float>(), m->g.ldz, gs.nb, gs.nx,
                                    sh.x0, stream_));
         launches_ += 1;
@@ -562,10 +573,19 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     if (!modelling && backward_only != 2) {
         const double upd = 2.0 * m->nt * (double)gs.nxe * gs.nze;
         times.cell_updates += upd;
-        const double s_b = (double)es;
         const double nint = (double)gs.nx * gs.nz;
-        times.algorithmic_bytes += 16.0 * upd + m->nsnap * nint * s_b + m->nsnap * nint * (s_b + 16.0) +
-                                   (double)sh.nrec * m->nt * 4.0;
+        if (recon_) {
+            // the source field's reverse steps over the interior and its band,
+            // the strips written forward and read backward, the image RMW
+            const double rev = (double)std::max(m->nt - 2, 0) * (gs.nx + 2.0 * m->half) * (gs.nz + 2.0 * m->half);
+            const double strips = 2.0 * std::max(m->nt - 1, 0) * (double)d.bsize * 4.0;
+            times.algorithmic_bytes += 16.0 * (upd + rev) + strips + m->nsnap * nint * (4.0 + 16.0) +
+                                       (double)sh.nrec * m->nt * 4.0;
+        } else {
+            const double s_b = (double)es;
+            times.algorithmic_bytes += 16.0 * upd + m->nsnap * nint * s_b + m->nsnap * nint * (s_b + 16.0) +
+                                       (double)sh.nrec * m->nt * 4.0;
+        }
         times.shots += 1;
     }
     if (m->t_start < 0) m->t_start = clock();
@@ -621,9 +641,28 @@ int Engine::build_tiles() {
         for (const auto& c : j.rec_cells) tflags[(size_t)(c.first / TX) * j.gs.ntz + c.second / kTileZ] = 1;
         auto& vec = by_half[j.m->half];
         const ShotDesc& d = host_descs_[(size_t)s];
+        // Reconstruction: tiles holding band cells store the strips forward; the
+        // source field's own tiles cover the interior and its band.
+        const int H = j.m->half, nb = j.gs.nb;
+        auto meets = [&](int tx, int tz, int xa, int xb, int za, int zb) {
+            return tx * TX < xb && tx * TX + TX > xa && tz * kTileZ < zb && tz * kTileZ + kTileZ > za;
+        };
+        const bool rec = (d.flags & kFlagRecon) != 0;
         for (int tz = 0; tz < j.gs.ntz; ++tz)
-            for (int tx = 0; tx < ntx; ++tx)
-                vec.push_back(make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0));
+            for (int tx = 0; tx < ntx; ++tx) {
+                TileRef r = make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0, nbuf_);
+                if (rec && (meets(tx, tz, nb - H, nb, nb, nb + j.gs.nz) ||
+                            meets(tx, tz, nb + j.gs.nx, nb + j.gs.nx + H, nb, nb + j.gs.nz) ||
+                            meets(tx, tz, nb, nb + j.gs.nx, nb - H, nb) ||
+                            meets(tx, tz, nb, nb + j.gs.nx, nb + j.gs.nz, nb + j.gs.nz + H)))
+                    r.flags |= kFlagBandTile;
+                vec.push_back(r);
+            }
+        if (rec)
+            for (int tz = 0; tz < j.gs.ntz; ++tz)
+                for (int tx = 0; tx < ntx; ++tx)
+                    if (meets(tx, tz, nb - H, nb + j.gs.nx + H, nb - H, nb + j.gs.nz + H))
+                        vec.push_back(make_tile_ref(d, s, tx, tz, TX, false, nbuf_, true));
         sig.push_back(s);
         sig.push_back(j.m->half);
         sig.push_back(ntx);
@@ -652,7 +691,8 @@ int Engine::build_tiles() {
     RTMB_CUDA(cudaStreamSynchronize(stream_));
     // Room for every slot's largest tile count (16-column tiles over the pool's
     // width), so that a wider shot mix does not regrow the list mid-run.
-    const size_t most = (size_t)nslots_ * (size_t)((nxe_cap_ + 15) / 16) * (size_t)((ldz_cap_ + kTileZ - 1) / kTileZ);
+    const size_t most = (size_t)nslots_ * (recon_ ? 2 : 1) * (size_t)((nxe_cap_ + 15) / 16) *
+                        (size_t)((ldz_cap_ + kTileZ - 1) / kTileZ);
     RTMB_CUDA(tiles_.reserve(std::max(all.size(), most) * sizeof(TileRef)));
     RTMB_CUDA(cudaMemcpy(tiles_.get(), all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
     for (auto& g : groups_) {
@@ -818,7 +858,8 @@ int Engine::run_steps(int steps) {
                 StepParams p{};
                 p.fields = pool_.get();
                 p.buf_stride = (long long)nxe_cap_ * ldz_cap_;
-                p.slot_stride = kFieldBuffers * p.buf_stride;
+                p.slot_stride = nbuf_ * p.buf_stride;
+                p.nbuf = nbuf_;
                 p.ldz = ldz_cap_;
                 p.ntiles = g.count;
                 p.descs = descs_.get<ShotDesc>();
@@ -1044,19 +1085,46 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
         snap_max = std::max(snap_max, b);
         snap_sum += b;
     }
-    const size_t per_slot = 2 * (size_t)g.nxe * g.ldz * elem() + (size_t)g.nx * g.lds * 16 +
+    const size_t per_slot = (size_t)(nbuf_ - 1) * g.nxe * g.ldz * elem() + (size_t)g.nx * g.lds * 16 +
                             (size_t)4 * g.nxe * 3 + (size_t)m.nt * 4 * 2048;
     int want = 1;
     if (cfg_.mode == RTM_B200_MODE_PLAIN && nshots > 1 &&
         2 * (per_slot + snap_max) + ((size_t)512 << 20) <= budget)
         want = 2;   // two shots staggered by one pass (run_queue)
+    InflightTune* tuning = nullptr;
+    int tuning_cand = -1;
     if (cfg_.mode != RTM_B200_MODE_PLAIN) {
-        // 32 shots per launch measured best on the 1150 x 400 workload (16: 4 %
-        // slower, 24: 7 %); the pool and the snapshot arena still bound it.
-        want = cfg_.max_shots_in_flight > 0 ? cfg_.max_shots_in_flight : 32;
-        want = std::min(want, std::max(nshots, 1));
         const size_t snap_avg = nshots > 0 ? snap_sum / (size_t)nshots : snap_max;
         const size_t fit = budget / std::max<size_t>(per_slot + snap_avg, 1);
+        if (cfg_.max_shots_in_flight > 0) {
+            want = cfg_.max_shots_in_flight;
+        } else {
+            // Tuned across calls: the candidates that fit memory and the survey
+            // run one per call on real work; then the fastest is kept.
+            const std::vector<long long> key = {g.nx, g.nz, m.half, m.nt, snap_type(), nshots};
+            for (auto& t : inflight_log_)
+                if (t.key == key) tuning = &t;
+            if (!tuning) {
+                InflightTune t;
+                t.key = key;
+                for (int c : {16, 32, 48, 64})
+                    if ((size_t)c <= fit && c <= std::max(nshots, 1)) t.cands.push_back(c);
+                if (t.cands.empty()) t.cands.push_back((int)std::max<size_t>(1, std::min<size_t>(fit, 16)));
+                t.shots_per_s.assign(t.cands.size(), 0.0);
+                if (t.cands.size() == 1) t.pick = t.cands[0];
+                inflight_log_.push_back(t);
+                tuning = &inflight_log_.back();
+            }
+            if (tuning->pick) {
+                want = tuning->pick;
+                tuning = nullptr;
+            } else {
+                for (size_t c = 0; c < tuning->cands.size(); ++c)
+                    if (tuning->shots_per_s[c] == 0.0) { tuning_cand = (int)c; break; }
+                want = tuning->cands[(size_t)tuning_cand];
+            }
+        }
+        want = std::min(want, std::max(nshots, 1));
         want = (int)std::max<size_t>(1, std::min<size_t>((size_t)want, fit));
     }
     RTMB_TRY(ensure_pool(want, g.nxe, g.ldz));
@@ -1094,6 +1162,17 @@ int Engine::migrate(const rtm_b200_shot* shots, int nshots, float* img, float* i
     float ms = 0;
     RTMB_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     times.kernel += ms * 1e-3;
+    if (tuning && ms > 0) {
+        tuning->shots_per_s[(size_t)tuning_cand] = nshots / (ms * 1e-3);
+        bool all = true;
+        for (double r : tuning->shots_per_s) all = all && r > 0.0;
+        if (all) {
+            size_t b = 0;
+            for (size_t c = 1; c < tuning->cands.size(); ++c)
+                if (tuning->shots_per_s[c] > tuning->shots_per_s[b]) b = c;
+            tuning->pick = tuning->cands[b];
+        }
+    }
     const auto t_d2h = std::chrono::steady_clock::now();
     stack_ready_ = true;
     RTMB_TRY(finalize_model_image(m, img, ill, img64, ill64));
@@ -1293,6 +1372,31 @@ int Engine::postprocess(float eps_relative, bool compensate_filtered, float* ill
     if (illum_out) RTMB_CUDA(cudaMemcpyAsync(illum_out, out_c, n * 4, cudaMemcpyDefault, stream_));
     if (filtered_out) RTMB_CUDA(cudaMemcpyAsync(filtered_out, out_f, n * 4, cudaMemcpyDefault, stream_));
     RTMB_CUDA(cudaStreamSynchronize(stream_));
+    return RTM_B200_OK;
+}
+
+int Engine::l2_probe(size_t bytes, int reps, double* gbps) {
+    if (!gbps || bytes < 4096 || reps < 1) return fail(RTM_B200_EINVAL, "probe needs >= 4 KiB and >= 1 pass");
+    RTMB_CUDA(cudaSetDevice(device_));
+    DevMem buf;
+    const size_t n = bytes / 16;
+    if (buf.alloc(n * 16 + 256) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RTM_B200_ENOMEM, "probe buffer");
+    }
+    RTMB_CUDA(cudaMemsetAsync(buf.get(), 0, n * 16 + 256, stream_));
+    const float4* src = buf.get<float4>();
+    float* sink = reinterpret_cast<float*>(buf.get<char>() + n * 16);
+    for (int i = 0; i < 3; ++i) RTMB_CUDA(launch_l2_read_probe(src, n, reps, -1.0f, sink, stream_));
+    RTMB_CUDA(cudaEventRecord(ev0_, stream_));
+    constexpr int kLaunches = 5;
+    for (int i = 0; i < kLaunches; ++i) RTMB_CUDA(launch_l2_read_probe(src, n, reps, -1.0f, sink, stream_));
+    RTMB_CUDA(cudaEventRecord(ev1_, stream_));
+    RTMB_CUDA(cudaEventSynchronize(ev1_));
+    float ms = 0;
+    RTMB_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    *gbps = (double)n * 16.0 * reps * kLaunches / (ms * 1e-3) / 1e9;
+    launches_ += 3 + kLaunches;
     return RTM_B200_OK;
 }
 

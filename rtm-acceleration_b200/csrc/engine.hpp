@@ -113,6 +113,7 @@ public:
     int drain();
 
     int memory_probe(size_t bytes, int iters, double* gbps);
+    int l2_probe(size_t bytes, int reps, double* gbps);
     double clock() const;
     int num_snapshots() const { return model_ ? model_->nsnap : 0; }
     long long snapshot_bytes() const;
@@ -167,6 +168,8 @@ private:
     rtm_b200_config cfg_{};
     bool f64_ = false;
     bool auto_arith_ = false;                // arithmetic AUTO: modelling runs IEEE
+    bool recon_ = false;                     // snapshot-free source reconstruction
+    int nbuf_ = kFieldBuffers;               // field buffers per slot
     bool modelling_now_ = false;             // inside model_shots
     bool exact() const {
         return cfg_.arithmetic == RTM_B200_ARITH_IEEE || (auto_arith_ && modelling_now_);
@@ -237,6 +240,15 @@ public:
         std::vector<double> us_per_step;
     };
     std::vector<TuneRecord> tune_log_;
+    // Shots in flight of the batch engine, tuned across migrate calls on the
+    // same survey: each early call runs one candidate on real work.
+    struct InflightTune {
+        std::vector<long long> key;          // grid, order, nt, snapshot type, shots
+        std::vector<int> cands;
+        std::vector<double> shots_per_s;     // measured (device time), 0 = untested
+        int pick = 0;                        // 0 until every candidate ran
+    };
+    std::vector<InflightTune> inflight_log_;
 private:
     // backpressure: at most kChunksInFlight chunks queued ahead of the GPU
     static constexpr int kChunksInFlight = 3;

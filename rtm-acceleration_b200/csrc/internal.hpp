@@ -4,11 +4,14 @@
 // Device layout (every array is "zfast", depth contiguous, like the reference's
 // index = ix*nz + iz, include/rtm_types.hpp:10-15 of the reference):
 //
-//   field pool   T[nslot][3][NXE][LDZ]  per shot slot: two time levels (the
+//   field pool   T[nslot][nbuf][NXE][LDZ]  per shot slot: two time levels (the
 //                leapfrog runs in place: p^{n+1} overwrites p^{n-1}) and the
-//                shot's (v dt)^2 on its extended grid; a shot's extended grid
-//                (nxe x nze) sits in the top-left corner of its slot.  LDZ is a
-//                multiple of 8 so every column starts on a 32-byte boundary.
+//                shot's (v dt)^2 on its extended grid; with source
+//                reconstruction two more levels (nbuf = 5) hold the receiver
+//                field of the backward pass while the first two hold the source
+//                field running backwards.  A shot's extended grid (nxe x nze)
+//                sits in the top-left corner of its slot.  LDZ is a multiple of
+//                8 so every column starts on a 32-byte boundary.
 //   vdt2 model   float[model_nx][LDZ]  (v dt)^2 for every interior model column,
 //                extended in depth by edge replication; a shot's slot copy is
 //                extended in x by clamping to its aperture window, which gives
@@ -16,6 +19,9 @@
 //                src/rtm/rtm_cpu.cpp:33-42 on the cropped model).
 //   snapshots    S[nsnap][nx][lds]  interior columns, rows [zs0, zs0+lds) of the
 //                extended grid (zs0 = nb rounded down to 4, lds multiple of 4).
+//   boundary     B[nt-1][bsize]  source reconstruction instead of snapshots:
+//   strips       level m = 1..nt-1 of the source field on the band of H cells
+//                around the interior (left, right: H x nz; top, bottom: nx x H).
 //   image/illum  A[nx][lds]          same layout as one snapshot.
 #pragma once
 #include <cstdint>
@@ -27,7 +33,7 @@ constexpr int kMaxHalf = 6;
 constexpr int kCoefSlots = 8;   // cx / cz entries in ShotDesc: kMaxHalf + 1, rounded up to a float4 pair
 constexpr int kTileZ = 128;          // rows per tile: 32 lanes x 4 consecutive rows
 
-enum SnapType : int { kSnapF32 = 0, kSnapBF16 = 1, kSnapF16 = 2, kSnapF64 = 3 };
+enum SnapType : int { kSnapF32 = 0, kSnapBF16 = 1, kSnapF16 = 2, kSnapF64 = 3, kSnapNone = 4 };
 enum AccMode : int {
     kAccPlain = 0,        // I += f*b straight into the shared image (reference order)
     kAccCompensated = 1,  // per-shot Kahan-compensated sums (sum, comp) pairs
@@ -36,6 +42,12 @@ enum ShotFlags : int {
     kFlagSnapshots = 1,   // forward pass stores snapshots
     kFlagImage = 2,       // backward pass runs (and images)
     kFlagRecord = 4,      // forward pass records traces at the receivers
+    kFlagRecon = 8,       // no snapshots: the forward pass stores the boundary
+                          // strips, the backward pass rebuilds the source field
+    kFlagSourceTile = 64, // TileRef only: a tile of the source field running
+                          // backwards (reconstruction), not of the shot's field
+    kFlagBandTile = 128,  // TileRef only: the tile holds cells of the boundary
+                          // strip band (reconstruction)
 };
 
 // One receiver cell of a shot: extended depth index and the receivers
@@ -55,7 +67,7 @@ struct ShotDesc {
     int win_nx;          // window width in model columns (== nx)
     int zs0, lds;        // snapshot/image row origin (extended z) and pitch
     int ntz;             // 128-row bands (stride of the snapshot scale exponents)
-    int pad1;
+    int bsize;           // reconstruction: boundary-strip cells per level
     // time
     int nt, si, nsnap;
     long long g0;        // global step at which forward step 0 runs
@@ -95,6 +107,24 @@ struct ShotDesc {
 };
 
 constexpr int kFieldBuffers = 3;     // p^n / p^{n+1}, p^{n-1}, (v dt)^2
+constexpr int kReconBuffers = 5;     // + the receiver field's two levels
+
+// Index of extended cell (x, z) in a boundary strip level, or -1 when the cell
+// is not in the band of H cells around the interior [nb, nb+nx) x [nb, nb+nz).
+#if defined(__CUDACC__)
+#define RTMB_HOST_DEVICE __host__ __device__
+#else
+#define RTMB_HOST_DEVICE
+#endif
+RTMB_HOST_DEVICE inline int strip_index(int x, int z, int nb, int nx, int nz, int H) {
+    const bool zin = z >= nb && z < nb + nz, xin = x >= nb && x < nb + nx;
+    if (zin && x >= nb - H && x < nb) return (x - (nb - H)) * nz + (z - nb);
+    if (zin && x >= nb + nx && x < nb + nx + H) return (H + x - (nb + nx)) * nz + (z - nb);
+    if (xin && z >= nb - H && z < nb) return 2 * H * nz + (x - nb) * H + (z - (nb - H));
+    if (xin && z >= nb + nz && z < nb + nz + H) return 2 * H * nz + (nx + x - nb) * H + (z - (nb + nz));
+    return -1;
+}
+inline int strip_cells(int nx, int nz, int H) { return 2 * H * (nx + nz); }
 
 // One receiver of a tile, staged in shared memory by the step kernel's producer.
 struct RecEntry {
@@ -125,7 +155,8 @@ struct TileRef {
 static_assert(sizeof(TileRef) == 80, "TileRef layout");
 
 // Host-side construction of a TileRef from the slot's descriptor.
-inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int tile_x, bool has_pts) {
+inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int tile_x, bool has_pts,
+                             int nbuf = kFieldBuffers, bool source_tile = false) {
     TileRef r{};
     r.slot = slot;
     r.tx = tx;
@@ -133,14 +164,14 @@ inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int ti
     r.has_pts = has_pts ? 1 : 0;
     r.x0 = tx * tile_x;
     r.z0 = tz * kTileZ;
-    r.field_base = d.field_slot * 3;
+    r.field_base = d.field_slot * nbuf;
     r.nt = d.nt;
     r.g0 = d.g0;
     r.total_steps = d.total_steps;
     r.si = d.si;
     r.wx = d.wx;
     r.wz = d.wz;
-    r.flags = d.flags;
+    r.flags = d.flags | (source_tile ? kFlagSourceTile : 0);
     r.nxe = d.nxe;
     r.nze = d.nze;
     r.has_src = d.src_x >= r.x0 && d.src_x < r.x0 + tile_x && d.src_z >= r.z0 && d.src_z < r.z0 + kTileZ;

@@ -522,6 +522,22 @@ cudaError_t launch_laplacian(const void* in, bool f64, int nx, int nz, double wx
     return cudaGetLastError();
 }
 
+__global__ void l2_read_probe_kernel(const float4* __restrict__ src, size_t n, int reps, float never,
+                                     float* sink) {
+    float acc = 0.f;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < reps; ++r)
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+            const float4 v = __ldcg(src + i);
+            acc += (v.x + v.y) + (v.z + v.w);
+        }
+    if (acc == never) sink[0] = acc;
+}
+cudaError_t launch_l2_read_probe(const float4* src, size_t n, int reps, float never, float* sink, cudaStream_t s) {
+    l2_read_probe_kernel<<<148 * 8, 256, 0, s>>>(src, n, reps, never, sink);
+    return cudaGetLastError();
+}
+
 __global__ void widen_kernel(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         dst[i] = (double)src[i];

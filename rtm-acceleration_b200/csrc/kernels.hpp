@@ -126,6 +126,11 @@ cudaError_t launch_extract_dense(const void* I, bool f64, int nx, int nz, int ld
 cudaError_t launch_laplacian(const void* in, bool f64, int nx, int nz, double wx, double wz, float* out,
                              cudaStream_t s);
 
+// Reads n float4 elements `reps` times in one launch, through L2 (no L1), and
+// folds them into a sum nothing uses unless it equals `never`: the L2 read
+// bandwidth of a buffer small enough to stay resident.
+cudaError_t launch_l2_read_probe(const float4* src, size_t n, int reps, float never, float* sink, cudaStream_t s);
+
 // float -> double widening of a dense array.
 cudaError_t launch_widen(const float* src, double* dst, size_t n, cudaStream_t s);
 

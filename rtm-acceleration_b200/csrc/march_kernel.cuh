@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kMarchThreads) march_kernel(const StepParams p
         __syncwarp();
         const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(W.desc);
 
-        T* base = reinterpret_cast<T*>(p.fields) + (size_t)(tr.field_base / kFieldBuffers) * p.slot_stride;
+        T* base = reinterpret_cast<T*>(p.fields) + (size_t)(tr.field_base / p.nbuf) * p.slot_stride;
         T* pc_buf = base + (size_t)ti.cur * p.buf_stride;          // p^n
         T* pn_buf = base + (size_t)(ti.cur ^ 1) * p.buf_stride;    // p^{n-1} in, p^{n+1} out
         const T* vd_buf = base + 2 * (size_t)p.buf_stride;         // (v dt)^2

@@ -251,6 +251,7 @@ int model_static(const rtm_b200_static_problem* pr, const rtm_b200_shot* shot, f
     p.fields = base + o_fields;
     p.buf_stride = (long long)buf_elems;
     p.slot_stride = (long long)kFieldBuffers * buf_elems;
+    p.nbuf = kFieldBuffers;
     p.ldz = g.ldz;
     p.ntiles = (int)ntiles;
     p.descs = reinterpret_cast<const ShotDesc*>(base + o_desc);

@@ -59,6 +59,7 @@ struct StepParams {
     int pdl;                        // host side: launch as a programmatic dependent launch
     int stall_tile;                 // failure-detection test: this tile is never produced (-1: none)
     int march_m;                    // march kernel: strip length in units of 2H+1 columns
+    int nbuf;                       // field buffers per slot (kFieldBuffers or kReconBuffers)
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -234,8 +235,8 @@ struct Halo {
 };
 
 // One shared-memory stage of the pipelined step kernel:
-//   [0, 64)       TileInfo: what the tile does this step (written by the producer)
-//   [64, ...)     the tile's ShotDesc
+//   [0, 128)      TileInfo: what the tile does this step (written by the producer)
+//   [128, ...)    the tile's ShotDesc
 //   [WX_OFF, ..)  taper weights wx of the tile's TX columns
 //   [WZ_OFF, ..)  taper weights wz of the tile's 128 rows
 //   [CS_OFF, ..)  receiver-cell offsets col_start[x0 .. x0+TX] (unstaged receivers)
@@ -250,8 +251,13 @@ struct alignas(16) TileInfo {
     int glog;   // log2 of the lanes per column of the band (step kernel)
     int plain;  // step kernel: no cell of the tile is masked, injects or records
     int unitw;  // step kernel: every live cell of the tile has sponge weight exactly 1
+    int prv;    // slot buffer holding p^{n-1} (written with p^{n+1}); cur holds p^n
+    int src;    // reconstruction, stored backward steps: slot buffer holding the
+                // source field at the imaged level (-1: images read snapshots)
+    int recon;  // a tile of the source field running backwards
+    int strip;  // forward pass with reconstruction: store the boundary strip
 };
-static_assert(sizeof(TileInfo) <= 64, "TileInfo fits its block of the stage header");
+static_assert(sizeof(TileInfo) <= 128, "TileInfo fits its block of the stage header");
 
 __host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v / 2); }
 
@@ -267,7 +273,7 @@ struct TileShape {
     static constexpr int PC_BYTES = SZ * SX * (int)sizeof(T);
     static constexpr int BOX_BYTES = kTileZ * TX * (int)sizeof(T);
     static constexpr int INFO_OFF = 0;
-    static constexpr int DESC_OFF = 64;
+    static constexpr int DESC_OFF = 128;
     static constexpr int WX_OFF = 512;
     static constexpr int WZ_OFF = WX_OFF + 128;
     static constexpr int CS_OFF = WZ_OFF + kTileZ * 4;
@@ -462,6 +468,28 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
                         }
                     }
                 }
+            }
+        }
+    }
+
+    if (!t.plain && (t.recon || t.strip)) {
+        // Source reconstruction.  A tile of the source field running backwards
+        // keeps its update on the interior, takes the band of H cells around it
+        // from the strip the forward pass stored for this level, and clears
+        // every other cell (nothing reads them).  A forward tile stores its
+        // band cells of level it+1 into that level's strip.
+        const int H_ = H;
+        const size_t lev = (size_t)(t.recon ? t.it - 2 : t.it) * (size_t)d.bsize;   // level - 1
+        float* strip = reinterpret_cast<float*>(d.snap) + lev;
+        const bool xin = x >= nb && x < nb + nx;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int z = zr + q;
+            const int bi = strip_index(x, z, nb, nx, d.nz, H_);
+            if (t.recon) {
+                if (!(xin && z >= nb && z < nb + d.nz)) val[q] = bi >= 0 ? (T)__ldg(strip + bi) : (T)0;
+            } else if (bi >= 0 && lane_in && col_live) {
+                stg1(strip + bi, (float)val[q]);
             }
         }
     }
@@ -738,7 +766,7 @@ __device__ __forceinline__ int first_item(const TileInfo& t, int tx, int warp) {
 template <int H, bool EXACT, int NCW, int TX>
 __device__ __forceinline__ void compute_tile_full_f32(const unsigned char* __restrict__ st, const TileInfo& t,
                                                       float* __restrict__ pcur, float* __restrict__ pnext,
-                                                      int ldz) {
+                                                      const float* __restrict__ psrc, int ldz) {
     using S = TileShape<float, H, NCW, TX>;
     constexpr int HP = S::HP;
     const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
@@ -824,7 +852,10 @@ __device__ __forceinline__ void compute_tile_full_f32(const unsigned char* __res
                 const uint32_t ic = (uint32_t)(x - nb) * (uint32_t)lds + (uint32_t)(zr - zs0);
                 const size_t cell = (size_t)t.ksnap * nx * lds + ic;
                 const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
-                load_snapshot4<float>(d, cell, eidx, fs);
+                if (psrc)   // reconstruction: the source field at the imaged level
+                    ldg4(psrc + (uint32_t)x * (uint32_t)ldz + zr, fs, 0);
+                else
+                    load_snapshot4<float>(d, cell, eidx, fs);
                 ldg4(reinterpret_cast<const float*>(d.img) + ic, Iv, 0);
                 ldg4(reinterpret_cast<const float*>(d.ill) + ic, Sv, 0);
             }
@@ -838,13 +869,14 @@ __device__ __forceinline__ void compute_tile_full_f32(const unsigned char* __res
 // Computes one tile after its boxes have landed in the stage.
 template <typename T, int H, bool EXACT, int NCW, int TX>
 __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ st, const TileInfo& t,
-                                             T* __restrict__ pcur, T* __restrict__ pnext, int ldz) {
+                                             T* __restrict__ pcur, T* __restrict__ pnext, const T* __restrict__ psrc,
+                                             int ldz) {
     // FP32 full bands take the column-pair path, except in the 8-warp x
     // 16-column shape: it runs 2 CTAs of 9 warps per SM at 96 registers per
     // thread, where the per-column path below fits without spilling.
     if constexpr (sizeof(T) == 4 && !(NCW == 8 && TX == 16)) {
         if (t.glog == 5) {   // full band: the column-pair path
-            compute_tile_full_f32<H, EXACT, NCW, TX>(st, t, pcur, pnext, ldz);
+            compute_tile_full_f32<H, EXACT, NCW, TX>(st, t, pcur, pnext, psrc, ldz);
             return;
         }
     }
@@ -904,7 +936,10 @@ __device__ __forceinline__ void compute_tile(const unsigned char* __restrict__ s
         if (do_image && lane_snap && col_int) {
             const size_t cell = (size_t)t.ksnap * nx * lds + ic;
             const size_t eidx = ((size_t)t.ksnap * nx + (x - nb)) * d.ntz + t.tz;
-            load_snapshot4<T>(d, cell, eidx, fs);
+            if (psrc)   // reconstruction: the source field at the imaged level
+                ldg4(psrc + (uint32_t)x * (uint32_t)ldz + zr, fs, 0);
+            else
+                load_snapshot4<T>(d, cell, eidx, fs);
             ldg4(reinterpret_cast<const T*>(d.img) + ic, Iv, 0);
             ldg4(reinterpret_cast<const T*>(d.ill) + ic, Sv, 0);
         }
@@ -991,6 +1026,37 @@ __device__ __forceinline__ TileInfo decode_tile(const TileRef& tr, long long g) 
     ti.ksnap = ks;
     const bool pts_matter = !ti.fwd || (tr.flags & kFlagRecord);
     ti.has_pts = pts_matter && tr.has_pts;
+    ti.prv = ti.cur ^ 1;
+    ti.src = -1;
+    if (tr.flags & kFlagSourceTile) {
+        // The source field run backwards during the backward pass of step it:
+        // level L(it) = 2 L(it+1) - L(it+2) + (v dt)^2 lap L(it+1) + injection of
+        // wavelet sample it+1, the forward update with the two levels swapped
+        // (level m lives in slot buffer m & 1).  L(nt) and L(nt-1) are what the
+        // forward pass left; L(0) is never imaged.
+        if (ti.fwd || ti.it < 1 || ti.it > nt - 2) {
+            ti.active = 0;
+            return ti;
+        }
+        ti.recon = 1;
+        ti.fwd = 1;            // injects like a forward step ...
+        ti.it = ti.it + 1;     // ... the wavelet sample of level it+1
+        ti.cur = ti.it & 1;
+        ti.prv = ti.cur ^ 1;
+        ti.first = 0;
+        ti.do_snap = ti.do_image = 0;
+        ti.has_pts = 0;
+        return ti;
+    }
+    if (tr.flags & kFlagRecon) {
+        if (ti.fwd) {
+            ti.strip = ti.it <= nt - 2;            // level it+1 of the source field
+        } else {                                   // receiver field in slot buffers 3, 4
+            ti.cur += 3;
+            ti.prv += 3;
+            ti.src = (ti.it + 1) & 1;              // the source field at level it+1
+        }
+    }
     return ti;
 }
 
@@ -1084,7 +1150,7 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
     // the ring of H zero cells on every side and holds no source or receiver
     // work this step.
     ti.plain = x0 >= H && x0 + S::TX <= nxe - H && z0 >= H && z0 + kTileZ <= tr.nze - H && !ti.has_pts &&
-               !(ti.fwd && tr.has_src);
+               !(ti.fwd && tr.has_src) && !ti.recon && !(ti.strip && (tr.flags & kFlagBandTile));
 
     constexpr int kDescWords = (int)(sizeof(ShotDesc) / 4);
     constexpr int kDescPerLane = (kDescWords + 31) / 32;
@@ -1116,7 +1182,7 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
         } else {
             mbar_expect_tx(full, S::PC_BYTES + 2 * S::BOX_BYTES);
             tma_load_3d(st + S::PC_OFF, map_pc, full, z0 - S::HP, x0 - H, tr.field_base + ti.cur);
-            tma_load_3d(st + S::PP_OFF, map_box, full, z0, x0, tr.field_base + (ti.cur ^ 1));
+            tma_load_3d(st + S::PP_OFF, map_box, full, z0, x0, tr.field_base + ti.prv);
         }
         tma_load_3d(st + S::VD_OFF, map_box, full, z0, x0, tr.field_base + 2);
     }
@@ -1149,7 +1215,7 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
     }
     // Stored backward steps: pull the tile's snapshot lines into L2 now, so the
     // consumers' snapshot loads a few tiles later hit L2 instead of HBM.
-    if (ti.do_image) {
+    if (ti.do_image && ti.src < 0) {
         const char* snap = reinterpret_cast<const char*>(sd.snap);
         const int snap_type = sd.snap_type, zs0 = sd.zs0, lds = sd.lds, nb = sd.nb, nx = sd.nx;
         const int es = (snap_type == kSnapF32) ? 4 : (snap_type == kSnapF64 ? 8 : 2);
@@ -1237,7 +1303,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, sizeof(T) == 8 ? 1 : (NCW == 4
                 const ShotDesc& d = *reinterpret_cast<const ShotDesc*>(st + S::DESC_OFF);
                 T* base = reinterpret_cast<T*>(p.fields) + (size_t)d.field_slot * p.slot_stride;
                 compute_tile<T, H, EXACT, NCW, TX>(st, info, base + (size_t)info.cur * p.buf_stride,
-                                                       base + (size_t)(info.cur ^ 1) * p.buf_stride, p.ldz);
+                                                       base + (size_t)info.prv * p.buf_stride,
+                                                       info.src >= 0 ? base + (size_t)info.src * p.buf_stride
+                                                                     : nullptr,
+                                                       p.ldz);
             }
             mbar_arrive(empty + s);
             if (++s == nst) { s = 0; phase ^= 1u; }

@@ -19,7 +19,7 @@ STATUS_NAMES = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", 
                 -6: "EUNSUPPORTED", -7: "EREJECTED", -8: "ENOTFOUND"}
 
 MODE_PLAIN, MODE_BATCH, MODE_SERVE = 0, 1, 2
-SNAP_F32, SNAP_BF16, SNAP_F16 = 0, 1, 2
+SNAP_F32, SNAP_BF16, SNAP_F16, SNAP_RECON = 0, 1, 2, 3
 ARITH_IEEE, ARITH_FMA, ARITH_FP64, ARITH_AUTO = 0, 1, 2, 3
 ACC_PLAIN, ACC_COMPENSATED = 0, 1
 
@@ -110,6 +110,7 @@ def load():
         "rtm_b200_clock": (C.c_double, [E]),
         "rtm_b200_memory_probe": (C.c_int, [E, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
         "rtm_b200_postprocess": (C.c_int, [E, C.c_float, C.c_int, vp, vp]),
+        "rtm_b200_l2_probe": (C.c_int, [E, C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
         "rtm_b200_model_shot_static": (C.c_int, [C.POINTER(StaticProblem), C.POINTER(Shot), vp, C.c_char_p,
                                                  C.c_size_t]),
     }

@@ -86,7 +86,7 @@ def shots_to_c(shots: Sequence[ShotRecord], keep: list):
 
 
 _MODES = {"plain": L.MODE_PLAIN, "batch": L.MODE_BATCH, "serve": L.MODE_SERVE}
-_SNAPS = {"f32": L.SNAP_F32, "bf16": L.SNAP_BF16, "f16": L.SNAP_F16}
+_SNAPS = {"f32": L.SNAP_F32, "bf16": L.SNAP_BF16, "f16": L.SNAP_F16, "recon": L.SNAP_RECON}
 _ARITH = {"ieee": L.ARITH_IEEE, "fma": L.ARITH_FMA, "fp64": L.ARITH_FP64, "auto": L.ARITH_AUTO}
 _ACC = {"plain": L.ACC_PLAIN, "compensated": L.ACC_COMPENSATED}
 
@@ -309,6 +309,12 @@ class Engine:
 
     def clock(self) -> float:
         return self.lib.rtm_b200_clock(self.h)
+
+    def l2_probe(self, nbytes: int = 24 << 20, reps: int = 40) -> float:
+        """L2 read bandwidth (GB/s) of an L2-resident nbytes buffer on the engine's GPU."""
+        g = C.c_double()
+        self._check(self.lib.rtm_b200_l2_probe(self.h, nbytes, reps, C.byref(g)), "l2_probe")
+        return g.value
 
     def memory_probe(self, nbytes: int, iters: int = 20) -> float:
         """Copy bandwidth (read+write GB/s) over an nbytes buffer on the engine's GPU."""
