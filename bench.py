@@ -437,6 +437,9 @@ def run_survey(args, workload):
     peak, peak_kind = read_peak()
     traffic = read_traffic()
     achieved = algo_rank / dev_time / 1e9
+    # per step launch, like the ncu figure: cells of an average launch
+    cells_per_launch = cell_updates(w, mine) * args.steps / max(launches, 1)
+    traffic_launch = traffic["bytes_per_cell_update"] * cells_per_launch if traffic else None
     line = {
         "metric": "shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_time / args.steps * 1e3, "higher_is_better": True,
@@ -454,7 +457,8 @@ def run_survey(args, workload):
         "gpu_launches": launches,
         "wall_s_timed": wall,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic.get("bytes_per_launch") if traffic else None, "peak_source": peak_kind,
+                     "traffic": traffic_launch, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_rank / max(launches, 1),
                      "algorithmic_bytes_per_step": algo_rank / args.steps, "l2_read_gbs": l2_gbs},
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},

@@ -175,7 +175,7 @@ int rtm_b200_autotune_report(const rtm_b200_engine* h, char* buf, size_t len) {
         auto choice = [](const rtmb::Engine::TuneChoice& c) {
             return std::string("{\"kernel\": \"") + (c.kind == 1 ? "march" : "ring") + "\", \"warps\": " +
                    std::to_string(c.warps) + ", \"tile_x\": " + std::to_string(c.tile_x) + ", \"stages\": " + std::to_string(c.stages) + ", \"march_m\": " +
-                   std::to_string(c.march_m) + "}";
+                   std::to_string(c.march_m) + ", \"spare\": " + std::to_string(c.spare) + "}";
         };
         js += "], \"candidates\": [";
         for (size_t k = 0; k < r.cands.size(); ++k) js += (k ? ", " : "") + choice(r.cands[k]);

@@ -290,6 +290,7 @@ StepVariant Engine::variant(int half) const {
     v.half = half;
     v.tile_x = tile_x_;
     v.warps = f64_ ? 8 : warps_;
+    v.spare = spare_ != 0 && step_ctas_per_sm(v) > 1;
     v.exact = exact();
     v.kind = (f64_ || recon_) ? kStepRing : kind_;   // the march kernel has no reconstruction
     v.march_m = march_m_;
@@ -673,6 +674,7 @@ int Engine::build_tiles() {
     }
     sig.push_back(tile_x_);
     sig.push_back(warps_);
+    sig.push_back(spare_);
     sig.push_back(exact() ? 1 : 0);
     sig.push_back(stage_override_);
     sig.push_back(kind_);
@@ -773,10 +775,11 @@ int Engine::run_chunk(int steps) {
         auto hit = tuned_.find(key);
         auto apply = [&](const TuneChoice& c) {
             if (kind_ != c.kind || warps_ != c.warps || tile_x_ != c.tile_x || stage_override_ != c.stages ||
-                march_m_ != c.march_m)
+                march_m_ != c.march_m || spare_ != c.spare)
                 tiles_dirty_ = true;
             kind_ = c.kind;
             warps_ = c.warps;
+            spare_ = c.spare;
             tile_x_ = c.tile_x;
             stage_override_ = c.stages;
             march_m_ = c.march_m;
@@ -788,10 +791,14 @@ int Engine::run_chunk(int steps) {
             // register-march strip lengths.  The march kernel's FMA arithmetic
             // is not the ring kernel's, so with FMA it is not a candidate: every
             // candidate of a mix must compute the same cells.
-            std::vector<TuneChoice> cands = {{kStepRing, 4, 16, 0, 3}, {kStepRing, 8, 16, 0, 3},
-                                             {kStepRing, 8, 32, 0, 3}};
+            // spare = 1: the grid leaves one CTA slot per SM free, so the next
+            // (programmatic dependent) step's CTAs are resident and waiting
+            // before this step ends: it pays when steps are short.
+            std::vector<TuneChoice> cands = {{kStepRing, 4, 16, 0, 3, 0}, {kStepRing, 4, 16, 0, 3, 1},
+                                             {kStepRing, 8, 16, 0, 3, 0}, {kStepRing, 8, 16, 0, 3, 1},
+                                             {kStepRing, 8, 32, 0, 3, 0}};
             if (exact())
-                for (int m : {2, 3, 5}) cands.push_back({kStepMarch, 8, 16, 0, m});
+                for (int m : {2, 3, 5}) cands.push_back({kStepMarch, 8, 16, 0, m, 0});
             if (pin_kind_ >= 0) {
                 std::vector<TuneChoice> keep;
                 for (const auto& c : cands)

@@ -217,6 +217,7 @@ private:
     int launches_ = 0;
     int tile_x_ = 16;                        // ring kernel: tile width (16 or 32 columns)
     int warps_ = 4;                          // ring kernel: consumer warps per CTA
+    int spare_ = 0;                          // ring kernel: leave one CTA slot per SM free
     int stage_override_ = 0;                 // ring kernel: pipeline stages (0 = default)
     int stall_tile_ = -1;                    // failure-detection test hook (RTM_B200_STALL_TILE)
     // Autotuner: the fastest step kernel and parameters measured on real steps,
@@ -226,7 +227,7 @@ private:
     int march_m_ = 3;                        // march strip length, units of 2H+1 columns
     int pin_kind_ = -1;                      // step kernel pinned by RTM_B200_STEP_KERNEL (-1: tuned)
 public:
-    struct TuneChoice { int kind, warps, tile_x, stages, march_m; };
+    struct TuneChoice { int kind, warps, tile_x, stages, march_m, spare; };
 private:
     std::map<std::vector<long long>, TuneChoice> tuned_;
     std::vector<long long> tune_key() const;

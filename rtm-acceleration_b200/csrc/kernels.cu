@@ -69,8 +69,17 @@ cudaError_t launch_impl(const CUtensorMap& mpc, const CUtensorMap& mpp, const St
     using S = TileShape<T, H, NCW, TX>;
     const cudaError_t e = attr_impl<T, H, EX, NCW, TX>();
     if (e != cudaSuccess) return e;
-    const int cap = max_grid_impl<T, H, EX, NCW, TX>(p.nstage);
+    int cap = max_grid_impl<T, H, EX, NCW, TX>(p.nstage);
     if (cap <= 0) return cudaErrorInvalidConfiguration;
+    if (p.spare) {   // one CTA slot per SM stays free for the next step's CTAs
+        static int sms = 0;
+        if (!sms) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        }
+        if (cap > sms) cap -= sms;
+    }
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)(p.ntiles < cap ? p.ntiles : cap));
     cfg.blockDim = dim3((NCW + 1) * 32);
@@ -228,6 +237,7 @@ cudaError_t launch_step(const StepVariant& v, const CUtensorMap& mpc, const CUte
     StepParams p = pin;
     p.nstage = v.nstage;
     p.march_m = v.march_m;
+    p.spare = v.spare ? 1 : 0;
     if (v.kind == kStepMarch) return v.exact ? march_by_half<true>(v.half, p, s) : march_by_half<false>(v.half, p, s);
     return dispatch<LaunchF>(v, cudaErrorInvalidValue, mpc, mpp, p, s);
 }

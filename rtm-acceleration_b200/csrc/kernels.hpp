@@ -16,6 +16,7 @@ struct StepVariant {
     bool exact = true;  // IEEE unfused float arithmetic (bit-identical path)
     int tile_x = 16;    // ring kernel: tile of 128 rows x tile_x (16 or 32) columns
     int warps = 8;      // ring kernel: consumer warps per CTA (see step_shape_supported)
+    bool spare = false; // ring kernel: grid leaves one CTA slot per SM free (shapes of 2+ CTAs/SM)
     int nstage = 3;     // shared-memory pipeline stages, 2..kMaxStages
     int kind = 0;       // 0: TMA ring kernel (step_kernel); 1: register march (march_kernel, FP32)
     int march_m = 3;    // march: strip length in units of 2*half+1 columns (1..9)

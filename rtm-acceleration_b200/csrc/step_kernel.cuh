@@ -60,6 +60,8 @@ struct StepParams {
     int stall_tile;                 // failure-detection test: this tile is never produced (-1: none)
     int march_m;                    // march kernel: strip length in units of 2H+1 columns
     int nbuf;                       // field buffers per slot (kFieldBuffers or kReconBuffers)
+    int spare;                      // ring kernel: leave one CTA slot per SM free, so that the
+                                    // next step's CTAs become resident before this step ends
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -1106,6 +1108,31 @@ __device__ __forceinline__ bool stage_receivers(const ShotDesc& sd, const TileIn
     return true;
 }
 
+// What the producer loads for a tile that does not depend on the step: the
+// tile's shot descriptor words, its taper weights.  Loaded for a CTA's first
+// tile before griddepcontrol.wait, so that their latency overlaps the previous
+// step's tail.
+constexpr int kDescWords = (int)(sizeof(ShotDesc) / 4);
+constexpr int kDescPerLane = (kDescWords + 31) / 32;
+struct TileStatic {
+    int dw[kDescPerLane];
+    float wxv;
+    float4 wzv;
+};
+
+template <int TX>
+__device__ __forceinline__ void load_tile_static(const StepParams& p, const TileRef& tr, TileStatic& ts) {
+    const int lane = threadIdx.x & 31;
+    const int* src = reinterpret_cast<const int*>(p.descs + tr.slot);
+#pragma unroll
+    for (int k = 0; k < kDescPerLane; ++k)
+        ts.dw[k] = lane + 32 * k < kDescWords ? __ldg(src + lane + 32 * k) : 0;
+    const int xw = tr.x0 + lane;
+    ts.wxv = (lane < TX && xw < tr.nxe) ? __ldg(tr.wx + xw) : 0.f;
+    ts.wzv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tr.z0 + 4 * lane < tr.nze) ts.wzv = __ldg(reinterpret_cast<const float4*>(tr.wz + tr.z0 + 4 * lane));
+}
+
 // Fills one stage with tile `t` (producer warp, all 32 lanes).  Lane 0 decodes
 // what the tile does this step and publishes it as TileInfo; the lanes copy
 // the shot descriptor, the tile's taper weights and (for tiles with receiver
@@ -1123,7 +1150,7 @@ __device__ __forceinline__ bool stage_receivers(const ShotDesc& sd, const TileIn
 template <typename T, int H, int NCW, int TX>
 __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, const CUtensorMap* map_pc,
                                              const CUtensorMap* map_box, const StepParams& p, const TileRef& tr,
-                                             long long g) {
+                                             long long g, const TileStatic* pre) {
     using S = TileShape<T, H, NCW, TX>;
     static_assert(S::TX <= 32, "one producer lane per tile column");
     static_assert(kTileZ == 4 * 32, "one float4 of the z taper per producer lane");
@@ -1152,19 +1179,15 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
     ti.plain = x0 >= H && x0 + S::TX <= nxe - H && z0 >= H && z0 + kTileZ <= tr.nze - H && !ti.has_pts &&
                !(ti.fwd && tr.has_src) && !ti.recon && !(ti.strip && (tr.flags & kFlagBandTile));
 
-    constexpr int kDescWords = (int)(sizeof(ShotDesc) / 4);
-    constexpr int kDescPerLane = (kDescWords + 31) / 32;
-    int dw[kDescPerLane];
-    {
-        const int* src = reinterpret_cast<const int*>(p.descs + tr.slot);
-#pragma unroll
-        for (int k = 0; k < kDescPerLane; ++k)
-            dw[k] = lane + 32 * k < kDescWords ? __ldg(src + lane + 32 * k) : 0;
-    }
+    TileStatic ts;
+    if (pre)
+        ts = *pre;
+    else
+        load_tile_static<S::TX>(p, tr, ts);
+    const int* dw = ts.dw;
     const int xw = x0 + lane;
-    const float wxv = (lane < S::TX && xw < nxe) ? __ldg(tr.wx + xw) : 0.f;
-    float4 wzv = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (z0 + 4 * lane < tr.nze) wzv = __ldg(reinterpret_cast<const float4*>(tr.wz + z0 + 4 * lane));
+    const float wxv = ts.wxv;
+    const float4 wzv = ts.wzv;
     // Sponge weight exactly 1 on every live cell of the tile (its live columns
     // and rows): the consumers then skip the weight multiplies.
     {
@@ -1270,14 +1293,21 @@ __global__ void __launch_bounds__((NCW + 1) * 32, sizeof(T) == 8 ? 1 : (NCW == 4
         fence_mbar_init();
     }
     __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    // The producer's first tile: its reference, descriptor and tapers do not
+    // depend on the previous step, so they load before the wait below.
+    TileRef cur{};
+    TileStatic first{};
+    if (warp == NCW) {
+        cur = p.tiles[blockIdx.x];
+        load_tile_static<S::TX>(p, cur, first);
+    }
     griddep_wait();
     griddep_launch_dependents();
     const long long g = *p.step_counter + p.step_offset;
-    const int warp = threadIdx.x >> 5;
 
     if (warp == NCW) {
         int s = 0, round = 0;   // stage and how many times the ring has wrapped
-        TileRef cur = p.tiles[blockIdx.x];
         TileRef nxt = cur;
         for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
             if (t + (int)gridDim.x < p.ntiles) nxt = p.tiles[t + gridDim.x];   // in flight while we wait
@@ -1286,7 +1316,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, sizeof(T) == 8 ? 1 : (NCW == 4
             // consumers' bounded wait run out (no copy is in flight for it).
             if (t != p.stall_tile) {
                 produce_tile<T, H, NCW, TX>(stages + (size_t)s * S::STAGE, full + s, &map_pc, &map_box, p, cur,
-                                                g);
+                                                g, t == (int)blockIdx.x ? &first : nullptr);
                 if ((threadIdx.x & 31) == 0) issued[s] = round + 1;
             }
             cur = nxt;
