@@ -555,6 +555,8 @@ def run_config1(args):
         mute_direct_wave(sh, w.mute_v, t_pad, t_pad)
     p = RTMParams(nb=w.nb, order=w.order, f0=w.f0, store_interval=w.store_interval)
     res, imgs = {}, {}
+    sampler = ClockSampler(dev)
+    sampler.start()
     for name, mode in (("plain", "plain"), ("batch", "batch")):
         with Engine(mode, p, device=dev) as e:
             e.setup(w.vel, w.nx, w.nz, w.dx, w.dz, nt=w.nt, dt=w.dt)
@@ -565,6 +567,7 @@ def run_config1(args):
             res[name] = {"shots_per_s": len(w.shots) / t["kernel"], "gcell_updates_per_s":
                          t["cell_updates"] / t["kernel"] / 1e9, "seconds": t["kernel"]}
             imgs[name] = img
+    sampler.stop()
     cpu = {}
     if os.path.exists(REF_RTM):
         with tempfile.TemporaryDirectory() as td:
@@ -590,6 +593,7 @@ def run_config1(args):
                             "batch_vs_reference": metrics.compare_images(ref_img, imgs["batch"])}
     print(json.dumps({"workload": "config1", "metric": "shots/s", "unit": "shots/s", "higher_is_better": True,
                       "value": res["plain"]["shots_per_s"], "b200": res, "reference_cpu": cpu,
+                      "clocks": sampler.summary(),
                       "data": "synthetic (the reference's generator recipe, GPU-modelled traces)",
                       "config": {"grid": "201x151 @10 m", "shots": 4, "nt": 1400, "order": 8, "store": 2,
                                  "mute": 1500}}))
