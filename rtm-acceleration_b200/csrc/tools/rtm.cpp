@@ -11,6 +11,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "options.hpp"
 #include "rtm_b200_engine.hpp"
 
 using namespace rtm_b200;
@@ -31,76 +32,57 @@ static void usage() {
         "  --illumination  --filter laplacian  --write-illum-map\n"
         "  --benchmark PATH  --benchmark-csv PATH  --dataset NAME\n"
         "  --segy-src-depth M (10)  --segy-rec-depth M (10)  --quiet\n"
-        "  --snap-precision f32|bf16|f16  --arith auto|ieee|fma|fp64  --max-in-flight N  --tile-cols 0|16|32\n"
+        "  --snap-precision f32|bf16|f16|recon  --arith auto|ieee|fma|fp64  --max-in-flight N  --tile-cols 0|16|32\n"
         "  --check-inputs         read and validate the inputs, print a summary, exit\n");
 }
+
+// Which velocity-header fields were set on the command line; those win over the
+// sidecar header.
+struct GivenHeaderFields {
+    bool nx = false, nz = false, dx = false, dz = false, ox = false, oz = false, layout = false;
+};
 
 int main(int argc, char** argv) try {
     std::string vel_path, shots_path, out_path, hdr_path, filter = "none", engine_name = "b200";
     std::string bench_path, bench_csv, dataset;
     io::VelocityHeader vh;
+    GivenHeaderFields given;
     RTMParams par;
     B200Options opt;
     int gpus = 1, nt_override = 0, max_shots = 0;
-    bool have_nx = false, have_nz = false, have_dx = false, have_dz = false, have_ox = false, have_oz = false,
-         have_layout = false, want_illum = false, want_map = false, check_only = false;
+    bool want_illum = false, want_map = false, check_only = false;
     float mute_v = 0.0f, segy_sz = 10.0f, segy_rz = 10.0f;
-    for (int i = 1; i < argc; ++i) {
-        const std::string a = argv[i];
-        auto next = [&]() -> std::string {
-            if (i + 1 >= argc) throw std::runtime_error("missing value after " + a);
-            return argv[++i];
-        };
-        if (a == "--velocity") vel_path = next();
-        else if (a == "--shots") shots_path = next();
-        else if (a == "--output") out_path = next();
-        else if (a == "--vel-header") hdr_path = next();
-        else if (a == "--nx") { vh.nx = std::stoi(next()); have_nx = true; }
-        else if (a == "--nz") { vh.nz = std::stoi(next()); have_nz = true; }
-        else if (a == "--dx") { vh.dx = std::stof(next()); have_dx = true; }
-        else if (a == "--dz") { vh.dz = std::stof(next()); have_dz = true; }
-        else if (a == "--ox") { vh.ox = std::stof(next()); have_ox = true; }
-        else if (a == "--oz") { vh.oz = std::stof(next()); have_oz = true; }
-        else if (a == "--vel-layout") { vh.layout = next(); have_layout = true; }
-        else if (a == "--order") par.order = std::stoi(next());
-        else if (a == "--nb") par.nb = std::stoi(next());
-        else if (a == "--sponge-alpha") par.sponge_alpha = std::stof(next());
-        else if (a == "--f0") par.f0 = std::stof(next());
-        else if (a == "--store-interval") par.store_interval = std::stoi(next());
-        else if (a == "--nt") nt_override = std::stoi(next());
-        else if (a == "--max-shots") max_shots = std::stoi(next());
-        else if (a == "--mute-direct") mute_v = std::stof(next());
-        else if (a == "--illumination") want_illum = true;
-        else if (a == "--write-illum-map") want_map = true;
-        else if (a == "--filter") filter = next();
-        else if (a == "--benchmark") bench_path = next();
-        else if (a == "--benchmark-csv") bench_csv = next();
-        else if (a == "--dataset") dataset = next();
-        else if (a == "--segy-src-depth") segy_sz = std::stof(next());
-        else if (a == "--segy-rec-depth") segy_rz = std::stof(next());
-        else if (a == "--quiet") par.verbose = false;
-        else if (a == "--engine") engine_name = next();
-        else if (a == "--gpus") gpus = std::stoi(next());
-        else if (a == "--list-engines") {
-            for (const auto& n : list_engines()) std::printf("%s\n", n.c_str());
-            return 0;
-        } else if (a == "--snap-precision") {
-            const std::string v = next();
-            opt.snap_precision = v == "bf16" ? RTM_B200_SNAP_BF16 : v == "f16" ? RTM_B200_SNAP_F16 : RTM_B200_SNAP_F32;
-            if (v != "bf16" && v != "f16" && v != "f32") throw std::runtime_error("--snap-precision f32|bf16|f16");
-        } else if (a == "--arith") {
-            const std::string v = next();
-            if (v == "ieee") opt.arithmetic = RTM_B200_ARITH_IEEE;
-            else if (v == "fma") opt.arithmetic = RTM_B200_ARITH_FMA;
-            else if (v == "fp64") opt.arithmetic = RTM_B200_ARITH_FP64;
-            else if (v == "auto") opt.arithmetic = RTM_B200_ARITH_AUTO;
-            else throw std::runtime_error("--arith auto|ieee|fma|fp64");
-        } else if (a == "--max-in-flight") opt.max_shots_in_flight = std::stoi(next());
-        else if (a == "--tile-cols") opt.tile_cols = std::stoi(next());
-        else if (a == "--check-inputs") check_only = true;
-        else if (a == "--help" || a == "-h") { usage(); return 0; }
-        else throw std::runtime_error("unknown option: " + a);
+
+    cli::Options table;
+    table.text("--velocity", vel_path).text("--shots", shots_path).text("--output", out_path)
+        .text("--vel-header", hdr_path)
+        .integer("--nx", vh.nx, &given.nx).integer("--nz", vh.nz, &given.nz)
+        .real("--dx", vh.dx, &given.dx).real("--dz", vh.dz, &given.dz)
+        .real("--ox", vh.ox, &given.ox).real("--oz", vh.oz, &given.oz)
+        .text("--vel-layout", vh.layout, &given.layout)
+        .integer("--order", par.order).integer("--nb", par.nb).real("--sponge-alpha", par.sponge_alpha)
+        .real("--f0", par.f0).integer("--store-interval", par.store_interval)
+        .integer("--nt", nt_override).integer("--max-shots", max_shots).real("--mute-direct", mute_v)
+        .boolean("--illumination", want_illum).boolean("--write-illum-map", want_map).text("--filter", filter)
+        .text("--benchmark", bench_path).text("--benchmark-csv", bench_csv).text("--dataset", dataset)
+        .real("--segy-src-depth", segy_sz).real("--segy-rec-depth", segy_rz)
+        .boolean("--quiet", par.verbose, false)
+        .text("--engine", engine_name).integer("--gpus", gpus)
+        .choice("--snap-precision", opt.snap_precision,
+                {{"f32", RTM_B200_SNAP_F32}, {"bf16", RTM_B200_SNAP_BF16}, {"f16", RTM_B200_SNAP_F16},
+                 {"recon", RTM_B200_SNAP_RECON}})
+        .choice("--arith", opt.arithmetic,
+                {{"auto", RTM_B200_ARITH_AUTO}, {"ieee", RTM_B200_ARITH_IEEE}, {"fma", RTM_B200_ARITH_FMA},
+                 {"fp64", RTM_B200_ARITH_FP64}})
+        .integer("--max-in-flight", opt.max_shots_in_flight).integer("--tile-cols", opt.tile_cols)
+        .boolean("--check-inputs", check_only)
+        .terminal("--list-engines").terminal("--help").terminal("-h");
+    const std::string stop = table.parse(argc, argv);
+    if (stop == "--list-engines") {
+        for (const auto& n : list_engines()) std::printf("%s\n", n.c_str());
+        return 0;
     }
+    if (!stop.empty()) { usage(); return 0; }
     if (vel_path.empty() || shots_path.empty() || (out_path.empty() && !check_only)) {
         usage();
         throw std::runtime_error("--velocity, --shots and --output are required");
@@ -118,13 +100,15 @@ int main(int argc, char** argv) try {
         found = io::read_header_file(vel_path + ".hdr", side);
     }
     if (found) {
-        if (!have_nx) vh.nx = side.nx;
-        if (!have_nz) vh.nz = side.nz;
-        if (!have_dx) vh.dx = side.dx;
-        if (!have_dz) vh.dz = side.dz;
-        if (!have_ox) vh.ox = side.ox;
-        if (!have_oz) vh.oz = side.oz;
-        if (!have_layout) vh.layout = side.layout;
+        const io::VelocityHeader cli_values = vh;
+        vh = side;
+        if (given.nx) vh.nx = cli_values.nx;
+        if (given.nz) vh.nz = cli_values.nz;
+        if (given.dx) vh.dx = cli_values.dx;
+        if (given.dz) vh.dz = cli_values.dz;
+        if (given.ox) vh.ox = cli_values.ox;
+        if (given.oz) vh.oz = cli_values.oz;
+        if (given.layout) vh.layout = cli_values.layout;
     }
     VelocityModel model = io::read_velocity_raw(vel_path, vh);
     std::vector<ShotRecord> shots = io::read_shots(shots_path, segy_sz, segy_rz);

@@ -12,6 +12,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "options.hpp"
 #include "rtm_b200_engine.hpp"
 
 using namespace rtm_b200;
@@ -22,43 +23,28 @@ int main(int argc, char** argv) try {
     float dx = 10.0f, dz = 10.0f, dt = 0.001f, f0 = 12.0f, src_z = 20.0f, rec_z = 20.0f, rec_dx = 20.0f;
     float shot_x0 = -1.0f, shot_dx = -1.0f;
     io::VelocityHeader vh;
-    bool have_nx = false, have_nz = false, have_dx = false, have_dz = false;
-    for (int i = 1; i < argc; ++i) {
-        const std::string a = argv[i];
-        auto next = [&]() -> std::string {
-            if (i + 1 >= argc) throw std::runtime_error("missing value after " + a);
-            return argv[++i];
-        };
-        if (a == "--outdir") outdir = next();
-        else if (a == "--nx") { nx = std::stoi(next()); have_nx = true; }
-        else if (a == "--nz") { nz = std::stoi(next()); have_nz = true; }
-        else if (a == "--dx") { dx = std::stof(next()); have_dx = true; }
-        else if (a == "--dz") { dz = std::stof(next()); have_dz = true; }
-        else if (a == "--nt") nt = std::stoi(next());
-        else if (a == "--dt") dt = std::stof(next());
-        else if (a == "--f0") f0 = std::stof(next());
-        else if (a == "--nshots") nshots = std::stoi(next());
-        else if (a == "--order") order = std::stoi(next());
-        else if (a == "--nb") nb = std::stoi(next());
-        else if (a == "--rec-dx") rec_dx = std::stof(next());
-        else if (a == "--src-z") src_z = std::stof(next());
-        else if (a == "--rec-z") rec_z = std::stof(next());
-        else if (a == "--velocity") vel_path = next();
-        else if (a == "--vel-layout") vh.layout = next();
-        else if (a == "--shots-out") shots_out = next();
-        else if (a == "--shot-x0") shot_x0 = std::stof(next());
-        else if (a == "--shot-dx") shot_dx = std::stof(next());
-        else if (a == "--engine") engine_name = next();
-        else throw std::runtime_error("unknown option: " + a);
-    }
+    bool given_nx = false, given_nz = false, given_dx = false, given_dz = false;
+    cli::Options table;
+    table.text("--outdir", outdir)
+        .integer("--nx", nx, &given_nx).integer("--nz", nz, &given_nz)
+        .real("--dx", dx, &given_dx).real("--dz", dz, &given_dz)
+        .integer("--nt", nt).real("--dt", dt).real("--f0", f0).integer("--nshots", nshots)
+        .integer("--order", order).integer("--nb", nb)
+        .real("--rec-dx", rec_dx).real("--src-z", src_z).real("--rec-z", rec_z)
+        .text("--velocity", vel_path).text("--vel-layout", vh.layout).text("--shots-out", shots_out)
+        .real("--shot-x0", shot_x0).real("--shot-dx", shot_dx).text("--engine", engine_name);
+    table.parse(argc, argv);
     VelocityModel model;
     if (!vel_path.empty()) {
         io::VelocityHeader side;
         if (io::read_header_file(vel_path + ".hdr", side)) {
-            if (!have_nx) nx = side.nx;
-            if (!have_nz) nz = side.nz;
-            if (!have_dx) dx = side.dx;
-            if (!have_dz) dz = side.dz;
+            // Sizes on the command line win.  The sidecar's layout applies unless
+            // the command line asked for a layout other than the default zfast,
+            // and its origin always applies.
+            nx = given_nx ? nx : side.nx;
+            nz = given_nz ? nz : side.nz;
+            dx = given_dx ? dx : side.dx;
+            dz = given_dz ? dz : side.dz;
             if (vh.layout == "zfast") vh.layout = side.layout;
             vh.ox = side.ox;
             vh.oz = side.oz;
