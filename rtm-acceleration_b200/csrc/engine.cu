@@ -305,7 +305,7 @@ StepVariant Engine::variant(int half) const {
 
 int Engine::encode_map(int half, bool with_halo, CUtensorMap* out) {
     const StepVariant v = variant(half);
-    const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)nslots_ * nbuf_};
+    const cuuint64_t dims[3] = {(cuuint64_t)ldz_cap_, (cuuint64_t)nxe_cap_, (cuuint64_t)pool_buffers()};
     const cuuint64_t strides[2] = {(cuuint64_t)ldz_cap_ * elem(), (cuuint64_t)ldz_cap_ * nxe_cap_ * elem()};
     const cuuint32_t box[3] = {(cuuint32_t)(with_halo ? step_box_z(v) : kTileZ),
                                (cuuint32_t)(with_halo ? step_box_x(v) : step_tile_x(v)), 1};
@@ -328,7 +328,8 @@ int Engine::ensure_pool(int nslots, int nxe_cap, int ldz_cap) {
     nslots_ = std::max(nslots, nslots_);
     nxe_cap_ = std::max(nxe_cap, nxe_cap_);
     ldz_cap_ = ldz_cap;
-    const size_t bytes = (size_t)nslots_ * nbuf_ * nxe_cap_ * ldz_cap_ * elem();
+    shared_vd_uid_ = 0;
+    const size_t bytes = (size_t)pool_buffers() * nxe_cap_ * ldz_cap_ * elem();
     cudaError_t e = pool_.alloc(bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -340,6 +341,25 @@ int Engine::ensure_pool(int nslots, int nxe_cap, int ldz_cap) {
     host_descs_.assign((size_t)nslots_, ShotDesc{});
     RTMB_CUDA(descs_.alloc(sizeof(ShotDesc) * nslots_));
     RTMB_CUDA(cudaMemset(descs_.get(), 0, sizeof(ShotDesc) * nslots_));
+    tiles_dirty_ = true;
+    return RTM_B200_OK;
+}
+
+// Loads m's (v dt)^2 table into the pool's shared buffer (zero rows below the
+// table, as in a slot's copy), unless the buffer holds it already or an active
+// job of another model still reads it; in that case m's shots keep loading their
+// slot's copies.  Stream-ordered after every launch that read the old table.
+int Engine::share_model_vdt2(const Model* m) {
+    if (f64_ || shared_vd_uid_ == m->uid || m->g.nx > nxe_cap_ || m->g.ldz > ldz_cap_) return RTM_B200_OK;
+    for (const auto& j : jobs_)
+        if (j.active && j.m->uid == shared_vd_uid_) return RTM_B200_OK;
+    const size_t buf = (size_t)nxe_cap_ * ldz_cap_ * elem();
+    char* dst = pool_.get<char>() + (size_t)shared_vd_buf() * buf;
+    RTMB_CUDA(cudaMemsetAsync(dst, 0, buf, stream_));
+    RTMB_CUDA(cudaMemcpy2DAsync(dst, (size_t)ldz_cap_ * sizeof(float), m->vdt2.get<float>(),
+                                (size_t)m->g.ldz * sizeof(float), (size_t)m->g.ldz * sizeof(float), (size_t)m->g.nx,
+                                cudaMemcpyDeviceToDevice, stream_));
+    shared_vd_uid_ = m->uid;
     tiles_dirty_ = true;
     return RTM_B200_OK;
 }
@@ -561,6 +581,7 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
     // The slot's (v dt)^2 on the shot's extended grid (third field buffer).
+    RTMB_TRY(share_model_vdt2(m));
     {
         char* vbuf = pool_.get<char>() + ((size_t)s * nbuf_ + 2) * nxe_cap_ * ldz_cap_ * elem();
         RTMB_CUDA(launch_slot_vdt2(vbuf, f64_, ldz_cap_, gs.nxe, m->vdt2.get<float>(), m->g.ldz, gs.nb, gs.nx,
@@ -649,9 +670,19 @@ int Engine::build_tiles() {
             return tx * TX < xb && tx * TX + TX > xa && tz * kTileZ < zb && tz * kTileZ + kTileZ > za;
         };
         const bool rec = (d.flags & kFlagRecon) != 0;
+        // Tiles whose columns all lie inside the aperture window load (v dt)^2
+        // from the model's shared table (the same values as the slot's copy).
+        const bool shared_vd = !f64_ && shared_vd_uid_ != 0 && j.m->uid == shared_vd_uid_;
+        auto place_vd = [&](TileRef r) {
+            if (shared_vd && r.x0 >= d.nb && r.x0 + TX <= d.nb + d.win_nx) {
+                r.vd_x = r.x0 - d.nb + d.model_x0;
+                r.vd_buf = shared_vd_buf();
+            }
+            return r;
+        };
         for (int tz = 0; tz < j.gs.ntz; ++tz)
             for (int tx = 0; tx < ntx; ++tx) {
-                TileRef r = make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0, nbuf_);
+                TileRef r = place_vd(make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0, nbuf_));
                 if (rec && (meets(tx, tz, nb - H, nb, nb, nb + j.gs.nz) ||
                             meets(tx, tz, nb + j.gs.nx, nb + j.gs.nx + H, nb, nb + j.gs.nz) ||
                             meets(tx, tz, nb, nb + j.gs.nx, nb - H, nb) ||
@@ -663,7 +694,7 @@ int Engine::build_tiles() {
             for (int tz = 0; tz < j.gs.ntz; ++tz)
                 for (int tx = 0; tx < ntx; ++tx)
                     if (meets(tx, tz, nb - H, nb + j.gs.nx + H, nb - H, nb + j.gs.nz + H))
-                        vec.push_back(make_tile_ref(d, s, tx, tz, TX, false, nbuf_, true));
+                        vec.push_back(place_vd(make_tile_ref(d, s, tx, tz, TX, false, nbuf_, true)));
         sig.push_back(s);
         sig.push_back(j.m->half);
         sig.push_back(ntx);
@@ -671,6 +702,7 @@ int Engine::build_tiles() {
         sig.push_back(j.g0);
         sig.push_back(j.total);
         sig.push_back(d.flags);
+        sig.push_back(shared_vd ? shared_vd_buf() : -1);
     }
     sig.push_back(tile_x_);
     sig.push_back(warps_);

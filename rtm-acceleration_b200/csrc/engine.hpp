@@ -20,6 +20,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <deque>
 #include <map>
@@ -48,8 +49,15 @@ struct ShotData {
 // One velocity model + time axis + parameters, with its device tables and its
 // image accumulators.  setup() makes the engine's own model; every serving
 // request makes one.
+// Process-wide identity of a Model object, never reused (unlike its address).
+inline unsigned long long next_model_uid() {
+    static std::atomic<unsigned long long> n{0};
+    return ++n;
+}
+
 struct Model {
     long long id = 0;
+    unsigned long long uid = next_model_uid();
     GridDims g;                        // full model grid
     float dx = 0, dz = 0, ox = 0, oz = 0, dt = 0, f0 = 0, alpha = 0;
     int order = 0, half = 0, nt = 0, si = 1, nsnap = 0;
@@ -187,9 +195,15 @@ private:
     bool stack_ready_ = false;               // model_'s stack holds a finished migration
     DevMem post_;                            // post-processing scratch
 
-    // field pool: T[nslots][3][nxe_cap][ldz_cap]
+    // field pool: T[nslots][nbuf][nxe_cap][ldz_cap], then (FP32) one more
+    // buffer holding a model's (v dt)^2 table, which interior tiles of every shot
+    // on that model load instead of their slot's copy, so that it stays in L2
     DevMem pool_;
     int nslots_ = 0, nxe_cap_ = 0, ldz_cap_ = 0;
+    unsigned long long shared_vd_uid_ = 0;   // model whose table the shared buffer holds (0: none)
+    int shared_vd_buf() const { return nslots_ * nbuf_; }
+    int pool_buffers() const { return nslots_ * nbuf_ + (f64_ ? 0 : 1); }
+    int share_model_vdt2(const Model* m);
     struct MapPair { CUtensorMap pc, box; };
     std::map<int, MapPair> maps_;            // by (half, tile width): p^n box with halo; 128 x TX box
     std::vector<Slot> slots_;

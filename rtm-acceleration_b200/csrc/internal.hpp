@@ -138,7 +138,9 @@ struct RecEntry {
 // 80-byte load only (the descriptor and tables follow in parallel).
 struct TileRef {
     int slot;            // index into the descriptor array
-    int tx, tz;          // tile coordinates inside the shot's extended grid
+    int vd_x, vd_buf;    // where the tile's (v dt)^2 box is loaded from: column and
+                         // field-pool buffer (the slot's own copy, or the model's
+                         // table shared by every shot on that model)
     int has_pts;         // the tile holds receiver cells
     int x0, z0;          // first column and row of the tile
     int field_base;      // first field buffer of the shot's slot
@@ -159,12 +161,12 @@ inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int ti
                              int nbuf = kFieldBuffers, bool source_tile = false) {
     TileRef r{};
     r.slot = slot;
-    r.tx = tx;
-    r.tz = tz;
     r.has_pts = has_pts ? 1 : 0;
     r.x0 = tx * tile_x;
     r.z0 = tz * kTileZ;
     r.field_base = d.field_slot * nbuf;
+    r.vd_x = r.x0;
+    r.vd_buf = r.field_base + 2;
     r.nt = d.nt;
     r.g0 = d.g0;
     r.total_steps = d.total_steps;

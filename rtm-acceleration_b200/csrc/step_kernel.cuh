@@ -1020,7 +1020,7 @@ __device__ __forceinline__ TileInfo decode_tile(const TileRef& tr, long long g) 
     ti.cur = j & 1;
     ti.x0 = tr.x0;
     ti.z0 = tr.z0;
-    ti.tz = tr.tz;
+    ti.tz = tr.z0 / kTileZ;
     const int ks = ti.it / tr.si;
     const bool stored = ks * tr.si == ti.it;
     ti.do_snap = ti.fwd && stored && (tr.flags & kFlagSnapshots);
@@ -1207,7 +1207,7 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
             tma_load_3d(st + S::PC_OFF, map_pc, full, z0 - S::HP, x0 - H, tr.field_base + ti.cur);
             tma_load_3d(st + S::PP_OFF, map_box, full, z0, x0, tr.field_base + ti.prv);
         }
-        tma_load_3d(st + S::VD_OFF, map_box, full, z0, x0, tr.field_base + 2);
+        tma_load_3d(st + S::VD_OFF, map_box, full, z0, tr.vd_x, tr.vd_buf);
     }
     {
         int* dst = reinterpret_cast<int*>(st + S::DESC_OFF);
@@ -1236,25 +1236,37 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
             }
         if (lane == 0) reinterpret_cast<TileInfo*>(st + S::INFO_OFF)->rec_staged = staged ? 1 : 0;
     }
-    // Stored backward steps: pull the tile's snapshot lines into L2 now, so the
-    // consumers' snapshot loads a few tiles later hit L2 instead of HBM.
-    if (ti.do_image && ti.src < 0) {
-        const char* snap = reinterpret_cast<const char*>(sd.snap);
-        const int snap_type = sd.snap_type, zs0 = sd.zs0, lds = sd.lds, nb = sd.nb, nx = sd.nx;
-        const int es = (snap_type == kSnapF32) ? 4 : (snap_type == kSnapF64 ? 8 : 2);
+    // Stored backward steps: pull the tile's snapshot, image and illumination
+    // lines (and their compensation words) into L2 now, so that the consumers'
+    // loads of them a tile later hit L2 instead of HBM.
+    if (ti.do_image) {
+        const int zs0 = sd.zs0, lds = sd.lds, nb = sd.nb, nx = sd.nx;
         const int r0 = z0 > zs0 ? z0 : zs0;
         const int r1 = z0 + kTileZ < zs0 + lds ? z0 + kTileZ : zs0 + lds;
-        if (snap && r1 > r0) {
-            const int bytes = (r1 - r0) * es;
-            const int lpc = (bytes + 127) >> 7;
-            for (int idx = lane; idx < S::TX * lpc; idx += 32) {
-                const int c = idx / lpc, l = idx - c * lpc;
-                const int xi = x0 + c - nb;
-                if (xi < 0 || xi >= nx) continue;
-                const char* a = snap + (((size_t)ti.ksnap * nx + xi) * lds + (r0 - zs0)) * es + (size_t)l * 128;
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+        const bool comp = sd.acc_mode != kAccPlain;
+        const int snap_es = (sd.snap_type == kSnapF32) ? 4 : (sd.snap_type == kSnapF64 ? 8 : 2);
+        if (r1 > r0)
+#pragma unroll 1
+            for (int a = 0; a < 5; ++a) {
+                const char* base =
+                    a == 0 ? (ti.src < 0 && sd.snap ? reinterpret_cast<const char*>(sd.snap) +
+                                                          (size_t)ti.ksnap * nx * lds * snap_es
+                                                    : nullptr)
+                    : a == 1 ? reinterpret_cast<const char*>(sd.img)
+                    : a == 2 ? reinterpret_cast<const char*>(sd.ill)
+                    : a == 3 ? (comp ? reinterpret_cast<const char*>(sd.img_c) : nullptr)
+                             : (comp ? reinterpret_cast<const char*>(sd.ill_c) : nullptr);
+                const int es = a == 0 ? snap_es : (int)sizeof(T);
+                if (!base) continue;
+                const int lpc = ((r1 - r0) * es + 127) >> 7;
+                for (int idx = lane; idx < S::TX * lpc; idx += 32) {
+                    const int c = idx / lpc, l = idx - c * lpc;
+                    const int xi = x0 + c - nb;
+                    if (xi < 0 || xi >= nx) continue;
+                    const char* q = base + ((size_t)xi * lds + (r0 - zs0)) * es + (size_t)l * 128;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
+                }
             }
-        }
     }
     mbar_arrive(full);
 }
