@@ -48,6 +48,8 @@ def lib():
         dp = C.POINTER(C.c_double)
         _lib.oracle_migrate_f32.argtypes = [C.POINTER(OracleParams), fp, C.c_int, C.POINTER(OracleShot), fp, fp]
         _lib.oracle_migrate_f64.argtypes = [C.POINTER(OracleParams), fp, C.c_int, C.POINTER(OracleShot), dp, dp]
+        _lib.oracle_migrate_f32_sum64.argtypes = [C.POINTER(OracleParams), fp, C.c_int, C.POINTER(OracleShot), dp,
+                                                  dp]
         _lib.oracle_model_shot_f32.argtypes = [C.POINTER(OracleParams), fp, C.POINTER(OracleShot), fp]
         _lib.oracle_model_shot_f64.argtypes = [C.POINTER(OracleParams), fp, C.POINTER(OracleShot), dp]
         _lib.oracle_model_shots_f32.argtypes = [C.POINTER(OracleParams), fp, C.c_int, C.POINTER(OracleShot), fp, C.c_int]
@@ -103,6 +105,21 @@ def migrate(params, vel, shots, dtype=np.float32):
     fn = lib().oracle_migrate_f32 if dtype == np.float32 else lib().oracle_migrate_f64
     cv = _fp if dtype == np.float32 else _dp
     rc = fn(C.byref(op), _fp(v), len(shots), arr, cv(img), cv(ill))
+    if rc != 0:
+        raise ValueError(f"oracle migrate rejected the parameters (code {rc})")
+    return img, ill
+
+
+def migrate_sum64(params, vel, shots):
+    """migrate() with FP32 propagation and FP32 products (bit-identical to the
+    reference) but FP64 image and illumination sums."""
+    keep = []
+    op = make_params(params)
+    v = np.ascontiguousarray(vel, np.float32).ravel()
+    n = params.nx * params.nz
+    img = np.zeros(n, np.float64)
+    ill = np.zeros(n, np.float64)
+    rc = lib().oracle_migrate_f32_sum64(C.byref(op), _fp(v), len(shots), _shots(shots, keep), _dp(img), _dp(ill))
     if rc != 0:
         raise ValueError(f"oracle migrate rejected the parameters (code {rc})")
     return img, ill

@@ -191,8 +191,11 @@ struct Problem {
     }
 
     // Reference backward.cpp:20-27 and :40-75 with imaging.cpp:25-40.
-    // trace_nt is the stride of the shot's traces (the shot's own nt).
-    void backward(const oracle_shot& s, int trace_nt, const T* snaps, T* img, T* ill) {
+    // trace_nt is the stride of the shot's traces (the shot's own nt).  The
+    // sums may be kept in a wider type A than the field (test use: FP32
+    // propagation and products, FP64 sums).
+    template <typename A>
+    void backward(const oracle_shot& s, int trace_nt, const T* snaps, A* img, A* ill) {
         std::vector<size_t> ridx((size_t)s.nrec);
         for (int ir = 0; ir < s.nrec; ++ir) ridx[ir] = cell(s.rx[ir], s.rz[ir]);
         zero();
@@ -210,8 +213,10 @@ struct Problem {
                     for (int iz = 0; iz < nz; ++iz) {
                         const size_t i = (size_t)ix * nz + iz;
                         const T fv = f[i];
-                        img[i] = img[i] + fv * pc[e(ix + nb, iz + nb)];
-                        ill[i] = ill[i] + fv * fv;
+                        const T pi = fv * pc[e(ix + nb, iz + nb)];
+                        const T si2 = fv * fv;
+                        img[i] = img[i] + (A)pi;
+                        ill[i] = ill[i] + (A)si2;
                     }
             }
         }
@@ -220,14 +225,14 @@ struct Problem {
 
 // Reference rtm.cpp:83-103: image/illum zeroed, forward + backward per shot,
 // one running image across shots.
-template <typename T>
+template <typename T, typename A = T>
 int migrate_impl(const oracle_params* p, const float* vel, int nshots,
-                 const oracle_shot* shots, T* image, T* illum) {
+                 const oracle_shot* shots, A* image, A* illum) {
     Problem<T> pr;
     const int rc = pr.setup(*p, vel);
     if (rc) return rc;
-    std::fill(image, image + pr.nint(), (T)0);
-    std::fill(illum, illum + pr.nint(), (T)0);
+    std::fill(image, image + pr.nint(), (A)0);
+    std::fill(illum, illum + pr.nint(), (A)0);
     std::vector<T> snaps((size_t)pr.nsnap * pr.nint(), (T)0);
     for (int is = 0; is < nshots; ++is) {
         const int trace_nt = shots[is].nt > 0 ? shots[is].nt : p->nt;
@@ -261,6 +266,10 @@ int oracle_migrate_f32(const oracle_params* p, const float* vel, int nshots,
 int oracle_migrate_f64(const oracle_params* p, const float* vel, int nshots,
                        const oracle_shot* shots, double* image, double* illum) {
     return migrate_impl<double>(p, vel, nshots, shots, image, illum);
+}
+int oracle_migrate_f32_sum64(const oracle_params* p, const float* vel, int nshots,
+                             const oracle_shot* shots, double* image, double* illum) {
+    return migrate_impl<float, double>(p, vel, nshots, shots, image, illum);
 }
 int oracle_model_shot_f32(const oracle_params* p, const float* vel,
                           const oracle_shot* shot, float* out) {

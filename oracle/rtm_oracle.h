@@ -56,6 +56,11 @@ int oracle_migrate_f32(const oracle_params* p, const float* vel, int nshots,
                        const oracle_shot* shots, float* image, float* illum);
 int oracle_migrate_f64(const oracle_params* p, const float* vel, int nshots,
                        const oracle_shot* shots, double* image, double* illum);
+/* The same with FP32 propagation and FP32 products, exactly as the reference,
+ * but the image and illumination summed in FP64: the reference point for the
+ * engines' compensated FP32 sums (test infrastructure only). */
+int oracle_migrate_f32_sum64(const oracle_params* p, const float* vel, int nshots,
+                             const oracle_shot* shots, double* image, double* illum);
 
 /* Forward modelling of one shot (reference RTMEngine::model_shot): writes
  * nrec*nt trace-major samples. */

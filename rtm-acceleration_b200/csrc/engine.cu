@@ -396,7 +396,7 @@ int Engine::ensure_slot(int s, const Model& m, const ShotData& sh, const GridDim
     if (modelling) RTMB_CUDA(sl.rec.reserve(sizeof(float) * nrec * m.nt));
     if (cfg_.mode != RTM_B200_MODE_PLAIN && !modelling) {
         const size_t n = std::max((size_t)gs.nx * gs.lds, (size_t)m.g.nx * m.g.lds);
-        RTMB_CUDA(sl.acc.reserve(f64_ ? 2 * n * 8 : 4 * n * 4));
+        RTMB_CUDA(sl.acc.reserve(f64_ ? 2 * n * 8 : 2 * n * 4 + 2 * n * 2));
     }
     return RTM_B200_OK;
 }
@@ -540,9 +540,10 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
         char* a = sl.acc.get<char>();
         d.img = a;
         d.ill = a + n_acc * elem();
+        // FP32 sums, then their BF16 compensation words (kAccCompensated)
         d.img_c = f64_ ? nullptr : a + 2 * n_acc * 4;
-        d.ill_c = f64_ ? nullptr : a + 3 * n_acc * 4;
-        RTMB_CUDA(cudaMemsetAsync(a, 0, f64_ ? 2 * n_acc * 8 : 4 * n_acc * 4, stream_));
+        d.ill_c = f64_ ? nullptr : a + 2 * n_acc * 4 + n_acc * 2;
+        RTMB_CUDA(cudaMemsetAsync(a, 0, f64_ ? 2 * n_acc * 8 : 2 * n_acc * 4 + 2 * n_acc * 2, stream_));
     }
     std::memcpy(st + o_desc, &d, sizeof(ShotDesc));
     host_descs_[(size_t)s] = d;
@@ -631,8 +632,8 @@ int Engine::finish_job(int s) {
             RTMB_CUDA(launch_stack_f64((const double*)d.img, (const double*)d.ill, m->img64.get<double>(),
                                        m->ill64.get<double>(), d.nx, d.lds, job.x0, stream_));
         else
-            RTMB_CUDA(launch_stack_f32((const float*)d.img, (const float*)d.img_c, (const float*)d.ill,
-                                       (const float*)d.ill_c, m->img64.get<double>(), m->ill64.get<double>(), d.nx,
+            RTMB_CUDA(launch_stack_f32((const float*)d.img, (const uint16_t*)d.img_c, (const float*)d.ill,
+                                       (const uint16_t*)d.ill_c, m->img64.get<double>(), m->ill64.get<double>(), d.nx,
                                        d.lds, job.x0, stream_));
         launches_ += 1;
     }

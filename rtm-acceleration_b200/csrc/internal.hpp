@@ -24,8 +24,9 @@
 //                around the interior (left, right: H x nz; top, bottom: nx x H).
 //   image/illum  A[nx][lds]          same layout as one snapshot.
 #pragma once
-#include <cstdint>
 #include <cstddef>
+#include <cstdint>
+#include <cstring>
 
 namespace rtmb {
 
@@ -102,7 +103,7 @@ struct ShotDesc {
     int8_t* snap_exp;        // nsnap * nx * ntz  power-of-two scale exponents
     void* img;               // nx * lds  (float, or double for T=double)
     void* ill;
-    void* img_c;             // compensation words (kAccCompensated)
+    void* img_c;             // Kahan compensation words, BF16 (kAccCompensated)
     void* ill_c;
 };
 
@@ -178,6 +179,18 @@ inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int ti
     r.nze = d.nze;
     r.has_src = d.src_x >= r.x0 && d.src_x < r.x0 + tile_x && d.src_z >= r.z0 && d.src_z < r.z0 + kTileZ;
     return r;
+}
+
+// The float value of a BF16 bit pattern (exact: BF16 is the top half of a float).
+RTMB_HOST_DEVICE inline float bf16_bits_to_float(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float f;
+    std::memcpy(&f, &u, sizeof f);
+    return f;
+#endif
 }
 
 // Error bits written by the kernels into the engine's device error word.

@@ -307,15 +307,15 @@ cudaError_t launch_insert_f64(const double* src, int nx, int nz, double* dst, in
 
 // ------------------------------------------------------------ FP64 stacking
 // Kahan pairs hold (sum, comp) with the running total = sum - comp.
-__global__ void stack_f32_kernel(const float* __restrict__ I, const float* __restrict__ Ic,
-                                 const float* __restrict__ S, const float* __restrict__ Sc, double* I64, double* S64,
-                                 int nx, int lds, int col0) {
+__global__ void stack_f32_kernel(const float* __restrict__ I, const uint16_t* __restrict__ Ic,
+                                 const float* __restrict__ S, const uint16_t* __restrict__ Sc, double* I64,
+                                 double* S64, int nx, int lds, int col0) {
     const size_t n = (size_t)nx * lds;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const size_t o = (size_t)col0 * lds + i;
         double vi = (double)I[i], vs = (double)S[i];
-        if (Ic) vi -= (double)Ic[i];
-        if (Sc) vs -= (double)Sc[i];
+        if (Ic) vi -= (double)bf16_bits_to_float(Ic[i]);
+        if (Sc) vs -= (double)bf16_bits_to_float(Sc[i]);
         I64[o] += vi;
         S64[o] += vs;
     }
@@ -330,7 +330,7 @@ __global__ void stack_f64_kernel(const double* __restrict__ I, const double* __r
     }
 }
 
-cudaError_t launch_stack_f32(const float* I, const float* Ic, const float* S, const float* Sc, double* I64,
+cudaError_t launch_stack_f32(const float* I, const uint16_t* Ic, const float* S, const uint16_t* Sc, double* I64,
                              double* S64, int nx, int lds, int col0, cudaStream_t s) {
     stack_f32_kernel<<<grid_for((size_t)nx * lds), 256, 0, s>>>(I, Ic, S, Sc, I64, S64, nx, lds, col0);
     return cudaGetLastError();

@@ -92,8 +92,9 @@ cudaError_t launch_insert_f64(const double* src, int nx, int nz, double* dst, in
                               cudaStream_t s);
 
 // FP64 cross-shot stack of one shot's image/illumination, shot columns placed
-// at model column `col0`.  comp arrays may be null (uncompensated sums).
-cudaError_t launch_stack_f32(const float* I, const float* Ic, const float* S, const float* Sc, double* I64,
+// at model column `col0`.  Ic / Sc are the Kahan compensation words (BF16 bit
+// patterns); they may be null (uncompensated sums).
+cudaError_t launch_stack_f32(const float* I, const uint16_t* Ic, const float* S, const uint16_t* Sc, double* I64,
                              double* S64, int nx, int lds, int col0, cudaStream_t s);
 cudaError_t launch_stack_f64(const double* I, const double* S, double* I64, double* S64, int nx, int lds,
                              int col0, cudaStream_t s);

@@ -156,6 +156,25 @@ __device__ __forceinline__ void ldg4(const double* p, double (&r)[4], int) {
 // 2^e as a float, exact for e in [-126, 127].
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
 
+// Four BF16 words (8 bytes, the compensation words of a 4-row group) to and
+// from T, rounding to nearest even on the way out.
+template <typename T>
+__device__ __forceinline__ void ldg_bf16x4(const uint16_t* p, T (&r)[4]) {
+    uint32_t a, b;
+    asm("ld.global.v2.u32 {%0, %1}, [%2];" : "=r"(a), "=r"(b) : "l"(gaddr(p)));
+    r[0] = (T)__uint_as_float(a << 16);
+    r[1] = (T)__uint_as_float(a & 0xffff0000u);
+    r[2] = (T)__uint_as_float(b << 16);
+    r[3] = (T)__uint_as_float(b & 0xffff0000u);
+}
+template <typename T>
+__device__ __forceinline__ void stg_bf16x4(uint16_t* p, const T (&r)[4]) {
+    const __nv_bfloat162 a = __floats2bfloat162_rn((float)r[0], (float)r[1]);
+    const __nv_bfloat162 b = __floats2bfloat162_rn((float)r[2], (float)r[3]);
+    asm volatile("st.global.v2.u32 [%0], {%1, %2};" ::"l"(gaddr(p)), "r"(*reinterpret_cast<const uint32_t*>(&a)),
+                 "r"(*reinterpret_cast<const uint32_t*>(&b)));
+}
+
 // ------------------------------------------------------- TMA and mbarriers
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -565,11 +584,16 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
                 }
             } else {
                 // Kahan: sum + (term - comp), comp tracks the lost low part.
-                T* imc = reinterpret_cast<T*>(d.img_c) + ic;
-                T* ilc = reinterpret_cast<T*>(d.ill_c) + ic;
+                // The compensation words are kept in BF16 (FP32 engines only):
+                // |comp| stays below about one ulp of the sum, so storing it
+                // with an 8-bit mantissa costs at most 2^-10 ulp(sum) per
+                // update, about 0.04 ulp after 2000 stored steps, and saves a
+                // quarter of a stored backward step's imaging traffic.
+                uint16_t* imc = reinterpret_cast<uint16_t*>(d.img_c) + ic;
+                uint16_t* ilc = reinterpret_cast<uint16_t*>(d.ill_c) + ic;
                 T Ic[4], Sc[4];
-                ldg4(imc, Ic, 0);
-                ldg4(ilc, Sc, 0);
+                ldg_bf16x4(imc, Ic);
+                ldg_bf16x4(ilc, Sc);
                 using E = Arith<T, true>;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -582,8 +606,8 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
                     Sc[q] = E::sub(E::sub(ts, Sv[q]), ys);
                     Sv[q] = ts;
                 }
-                stg4(imc, Ic);
-                stg4(ilc, Sc);
+                stg_bf16x4(imc, Ic);
+                stg_bf16x4(ilc, Sc);
             }
             stg4(img, Iv);
             stg4(ill, Sv);
@@ -1256,7 +1280,7 @@ __device__ __forceinline__ void produce_tile(unsigned char* st, uint64_t* full, 
                     : a == 2 ? reinterpret_cast<const char*>(sd.ill)
                     : a == 3 ? (comp ? reinterpret_cast<const char*>(sd.img_c) : nullptr)
                              : (comp ? reinterpret_cast<const char*>(sd.ill_c) : nullptr);
-                const int es = a == 0 ? snap_es : (int)sizeof(T);
+                const int es = a == 0 ? snap_es : (a >= 3 ? 2 : (int)sizeof(T));   // BF16 compensation words
                 if (!base) continue;
                 const int lpc = ((r1 - r0) * es + 127) >> 7;
                 for (int idx = lane; idx < S::TX * lpc; idx += 32) {

@@ -164,6 +164,22 @@ def test_batch_engine_vs_oracles(acc):
     assert rel_l2(ill64, ill) <= 1e-5
 
 
+def test_compensated_sums_match_fp64_sums_of_the_fp32_products():
+    """Batch engine with IEEE propagation (the reference's FP32 fields and
+    products, bit for bit): its per-shot Kahan sums (FP32 sums, BF16
+    compensation words) stacked in FP64 against FP64 sums of the same
+    products; the uncompensated FP32 sums for scale."""
+    p, v, shots = small_problem(order=8, nshots=3, si=1, nt=400)
+    ref_img, ref_ill = oracle.migrate_sum64(p, v, shots)
+    err = {}
+    for acc in ("compensated", "plain"):
+        with make_engine("batch", p, v, arithmetic="ieee", accumulation=acc, max_shots_in_flight=3) as e:
+            img, ill = e.migrate_f64(shots)
+        err[acc] = (rel_l2(ref_img, img), rel_l2(ref_ill, ill))
+    assert err["compensated"][0] <= 1e-8 and err["compensated"][1] <= 1e-8, err
+    assert err["compensated"][0] <= err["plain"][0] and err["compensated"][1] <= err["plain"][1], err
+
+
 @pytest.mark.parametrize("snap", ["bf16", "f16"])
 def test_reduced_precision_snapshots_within_1e3(snap):
     p, v, shots = small_problem(order=8, nshots=3, si=2)

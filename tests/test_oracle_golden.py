@@ -106,6 +106,17 @@ def test_fp64_oracle_is_the_same_scheme():
     assert rel_l2(s64, s32) < 1e-5
 
 
+def test_fp64_sum_oracle_shares_the_fp32_propagation():
+    """migrate_sum64 runs the FP32 scheme and only widens the sums: it sits
+    within FP32 rounding of the FP32 oracle, and its sums differ from the
+    FP32 ones."""
+    p, v, shots = random_problem(seed=5, order=8, nx=37, nz=29, nb=10, nt=120, si=1)
+    img32, ill32 = oracle.migrate(p, v, shots)
+    img, ill = oracle.migrate_sum64(p, v, shots)
+    assert rel_l2(img, img32) <= 1e-6 and rel_l2(ill, ill32) <= 1e-6
+    assert not np.array_equal(img.astype(np.float32), img32) or not np.array_equal(ill.astype(np.float32), ill32)
+
+
 def test_oracle_rejects_what_the_reference_rejects():
     p, v, shots = random_problem(seed=1, order=8, nx=20, nz=20, nb=8, nt=20, si=1)
     for bad in (dict(order=7), dict(nb=4), dict(store_interval=0), dict(nt=0)):
