@@ -136,6 +136,11 @@ int Engine::init() {
     RTMB_CUDA(cudaStreamSynchronize(stream_));
     tile_x_ = cfg_.tile_cols == 32 ? 32 : 16;
     warps_ = tile_x_ == 32 ? 8 : 4;
+    // Test hook: RTM_B200_RING_WARPS=8 with tile_cols 16 pins the 8-warp x
+    // 16-column shape (its per-column path), so tests can compare it with the
+    // column-pair shapes.
+    if (const char* w = std::getenv("RTM_B200_RING_WARPS"))
+        if (tile_x_ == 16 && cfg_.tile_cols != 0 && std::atoi(w) == 8) warps_ = 8;
     autotune_ = cfg_.tile_cols == 0;
     // Failure-detection test hook: the first step launch leaves this tile's
     // stage empty, so the kernel's bounded wait must give up and report.

@@ -2,10 +2,11 @@
 
 The autotuner picks the ring kernel's shape per job mix, so each shape has to
 compute the same cells: tile_cols 16 runs 4 consumer warps x 16-column tiles,
-tile_cols 32 runs 8 x 32.  The problem is tall enough for tiles that lie
-inside the zero ring and hold neither receivers nor the source (rows 128-255),
-which take the kernels' lean paths on unstored steps and, in the 8 x 32 shape,
-on stored backward steps.
+tile_cols 32 runs 8 x 32, and tile_cols 16 with RTM_B200_RING_WARPS=8 runs
+8 x 16, whose full bands take the per-column path and its general epilogue.
+The problem is tall enough for tiles that lie inside the zero ring and hold
+neither receivers nor the source (rows 128-255), which in the column-pair
+shapes take the lean paths of unstored and stored forward steps.
 
 Tolerances: the plain engine (IEEE arithmetic) is bit-identical to the oracle
 in every shape; the batch engine's images are bit-identical across shapes and
@@ -19,23 +20,33 @@ from helpers import bits_equal, make_engine, rel_l2, small_problem
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [16, 32]
+SHAPES = [(16, 4), (16, 8), (32, 8)]   # (tile_cols, consumer warps)
 
 
 @pytest.fixture
 def ring_only(monkeypatch):
     monkeypatch.setenv("RTM_B200_STEP_KERNEL", "ring")
+    return monkeypatch
+
+
+def shape_engine(monkeypatch, mode, p, v, shape, **kw):
+    tile_cols, warps = shape
+    if warps == 8 and tile_cols == 16:
+        monkeypatch.setenv("RTM_B200_RING_WARPS", "8")
+    else:
+        monkeypatch.delenv("RTM_B200_RING_WARPS", raising=False)
+    return make_engine(mode, p, v, tile_cols=tile_cols, **kw)
 
 
 def tall_problem():
     return small_problem(order=8, nx=150, nz=170, nb=50, nt=260, nshots=3, si=2)
 
 
-@pytest.mark.parametrize("tile_cols", SHAPES)
-def test_plain_every_shape_bit_exact_vs_oracle(ring_only, tile_cols):
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: f"{s[1]}x{s[0]}")
+def test_plain_every_shape_bit_exact_vs_oracle(ring_only, shape):
     p, v, shots = tall_problem()
     ref_img, ref_ill = oracle.migrate(p, v, shots)
-    with make_engine("plain", p, v, tile_cols=tile_cols) as e:
+    with shape_engine(ring_only, "plain", p, v, shape) as e:
         img, ill = e.migrate(shots)
     assert bits_equal(img, ref_img), rel_l2(ref_img, img)
     assert bits_equal(ill, ref_ill), rel_l2(ref_ill, ill)
@@ -46,12 +57,12 @@ def test_plain_every_shape_bit_exact_vs_oracle(ring_only, tile_cols):
 def test_batch_shapes_agree_bitwise(ring_only, snap, acc):
     p, v, shots = tall_problem()
     out = []
-    for tile_cols in SHAPES:
-        with make_engine("batch", p, v, tile_cols=tile_cols, snap=snap, accumulation=acc,
-                         max_shots_in_flight=3) as e:
+    for shape in SHAPES:
+        with shape_engine(ring_only, "batch", p, v, shape, snap=snap, accumulation=acc, max_shots_in_flight=3) as e:
             out.append(e.migrate(shots))
-    for a, b in zip(out[0], out[1]):
-        assert bits_equal(a, b), rel_l2(a, b)
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            assert bits_equal(a, b), rel_l2(a, b)
     ref64, ill64 = oracle.migrate(p, v, shots, np.float64)
     tol = 1e-5 if snap == "f32" else 1e-3
     assert rel_l2(ref64, out[0][0]) <= tol
