@@ -6,7 +6,7 @@ tile_cols 32 runs 8 x 32, and tile_cols 16 with RTM_B200_RING_WARPS=8 runs
 8 x 16, whose full bands take the per-column path and its general epilogue.
 The problem is tall enough for tiles that lie inside the zero ring and hold
 neither receivers nor the source (rows 128-255), which in the column-pair
-shapes take the lean paths of unstored and stored forward steps.
+shapes take the lean path of unstored steps.
 
 Tolerances: the plain engine (IEEE arithmetic) is bit-identical to the oracle
 in every shape; the batch engine's images are bit-identical across shapes and
