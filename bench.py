@@ -466,7 +466,9 @@ def run_survey(args, workload):
         "clocks": sampler.summary() if sampler else None,
     }
     if world == 1 and not args.no_extras:
-        line.update(survey_extras(args, w, p, snap, local, l2_gbs, value))
+        picks = [r.get("pick") for r in tune if r.get("kind") == "shots_in_flight" and r.get("pick")]
+        line.update(survey_extras(args, w, p, snap, local, l2_gbs, value,
+                                  picks[-1] if picks else (args.max_in_flight or 0)))
     if world == 1 and not args.no_cpu_baseline and workload == "config3" and os.path.exists(REF_RTM):
         threads = os.cpu_count() or 1
         vm = _velocity_models()
@@ -479,11 +481,13 @@ def run_survey(args, workload):
     print(json.dumps(line))
 
 
-def survey_extras(args, w, p, snap, dev, l2_gbs, batch_value):
+def survey_extras(args, w, p, snap, dev, l2_gbs, batch_value, inflight=0):
     """Single-GPU legs of the survey line: the plain FP32 engine on the same
     shots (its ratio to the batched engine and its L2 roofline), the image
     error of both against an FP64 run of the same scheme, and the order-12
-    survey."""
+    survey.  The order-12 batch leg runs at `inflight` shots in flight, the
+    count the order-8 survey's tuner kept (0: the engine's own choice), so that
+    its one timed call does not measure a tuning candidate."""
     from rtm_b200 import Engine, RTMParams, synth
     out = {}
     plain_shots = w.shots[:args.plain_shots] if args.plain_shots else w.shots
@@ -520,7 +524,7 @@ def survey_extras(args, w, p, snap, dev, l2_gbs, batch_value):
                 s.nt = args.nt
         _model_traces(w12, dev)
         p12 = RTMParams(nb=w12.nb, order=12, f0=w12.f0, store_interval=w12.store_interval)
-        with Engine("batch", p12, device=dev, snap=snap) as e:
+        with Engine("batch", p12, device=dev, snap=snap, max_shots_in_flight=inflight) as e:
             e.setup(w12.vel, w12.nx, w12.nz, w12.dx, w12.dz, nt=w12.nt, dt=w12.dt)
             _timed_migrate(e, w12.shots[:16])
             t = _timed_migrate(e, w12.shots)
