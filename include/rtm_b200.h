@@ -72,7 +72,8 @@ extern "C" {
 
 /* ---- accumulation of the per-shot image (batch/serve modes) ------------- */
 #define RTM_B200_ACC_PLAIN        0  /* running FP32 image, reference order    */
-#define RTM_B200_ACC_COMPENSATED  1  /* Kahan FP32 per shot + FP64 stack       */
+#define RTM_B200_ACC_COMPENSATED  1  /* Kahan FP32 per shot (BF16 compensation
+                                        words) + FP64 stack                   */
 
 typedef struct rtm_b200_engine rtm_b200_engine;
 
