@@ -141,6 +141,9 @@ int Engine::init() {
     // column-pair shapes.
     if (const char* w = std::getenv("RTM_B200_RING_WARPS"))
         if (tile_x_ == 16 && cfg_.tile_cols != 0 && std::atoi(w) == 8) warps_ = 8;
+    // Test hook: RTM_B200_BAND_SHIFT=0 keeps every job's bands at row 0, so tests
+    // can compare shifted and unshifted band origins bit for bit.
+    if (const char* b = std::getenv("RTM_B200_BAND_SHIFT")) band_shift_ = std::atoi(b) != 0;
     autotune_ = cfg_.tile_cols == 0;
     // Failure-detection test hook: the first step launch leaves this tile's
     // stage empty, so the kernel's bounded wait must give up and report.
@@ -297,7 +300,8 @@ StepVariant Engine::variant(int half) const {
     v.warps = f64_ ? 8 : warps_;
     v.spare = spare_ != 0 && step_ctas_per_sm(v) > 1;
     v.exact = exact();
-    v.kind = (f64_ || recon_) ? kStepRing : kind_;   // the march kernel has no reconstruction
+    // the march kernel has no reconstruction, nor shifted bands
+    v.kind = (f64_ || recon_ || shifted_bands()) ? kStepRing : kind_;
     v.march_m = march_m_;
     v.nstage = step_default_stages(v);
     if (stage_override_ > 0) {
@@ -407,6 +411,12 @@ int Engine::ensure_slot(int s, const Model& m, const ShotData& sh, const GridDim
 }
 
 // --------------------------------------------------------------- scheduling
+bool Engine::shifted_bands() const {
+    for (const auto& j : jobs_)
+        if (j.active && j.gs.z0 > 0) return true;
+    return false;
+}
+
 int Engine::active_jobs() const {
     int n = 0;
     for (const auto& j : jobs_) n += j.active ? 1 : 0;
@@ -421,6 +431,22 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     job.m = m;
     job.shot = shot;
     job.gs = make_grid(sh.wnx, m->g.nz, m->g.nb, m->half);
+    // Band origin.  The live rows are [H, nze - H); the rows outside stay zero
+    // (the reference's ring).  For the ring kernel's FMA migration jobs the
+    // 128-row bands start at s, the largest multiple of 4 not above H, when
+    // that covers the live rows with one band fewer: nze = 520 at order 8
+    // becomes four bands of rows 4-515 instead of five, the fifth holding 8
+    // rows, whose tiles cost nearly as much as full ones.  Sources and
+    // receivers sit at rows >= nb >= s.  The rows outside the bands are
+    // cleared once when the slot is set up and never written.
+    {
+        const int H = m->half, s0 = H & ~3;
+        const int ntz_s = (job.gs.nze - H - s0 + kTileZ - 1) / kTileZ;
+        if (band_shift_ && !modelling && !recon_ && !exact() && s0 > 0 && job.gs.nb >= s0 && ntz_s < job.gs.ntz) {
+            job.gs.z0 = s0;
+            job.gs.ntz = ntz_s;
+        }
+    }
     job.x0 = sh.x0;
     job.modelling = modelling;
     job.rec_host = rec_host;
@@ -586,6 +612,18 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                                 sizeof(ShotDesc));
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
+    // Rows outside a shifted job's bands: zero in both field levels.
+    if (gs.z0 > 0) {
+        const size_t pitch = (size_t)ldz_cap_ * elem();
+        const int below = gs.z0 + kTileZ * gs.ntz;
+        for (int b = 0; b < 2; ++b) {
+            char* fb = pool_.get<char>() + ((size_t)s * nbuf_ + b) * nxe_cap_ * ldz_cap_ * elem();
+            RTMB_CUDA(cudaMemset2DAsync(fb, pitch, 0, (size_t)gs.z0 * elem(), (size_t)nxe_cap_, stream_));
+            if (below < ldz_cap_)
+                RTMB_CUDA(cudaMemset2DAsync(fb + (size_t)below * elem(), pitch, 0, (size_t)(ldz_cap_ - below) * elem(),
+                                            (size_t)nxe_cap_, stream_));
+        }
+    }
     // The slot's (v dt)^2 on the shot's extended grid (third field buffer).
     RTMB_TRY(share_model_vdt2(m));
     {
@@ -666,7 +704,8 @@ int Engine::build_tiles() {
         const int TX = step_tile_x(variant(j.m->half));
         const int ntx = (j.gs.nxe + TX - 1) / TX;
         std::vector<uint8_t> tflags((size_t)ntx * j.gs.ntz, 0);
-        for (const auto& c : j.rec_cells) tflags[(size_t)(c.first / TX) * j.gs.ntz + c.second / kTileZ] = 1;
+        for (const auto& c : j.rec_cells)
+            tflags[(size_t)(c.first / TX) * j.gs.ntz + (c.second - j.gs.z0) / kTileZ] = 1;
         auto& vec = by_half[j.m->half];
         const ShotDesc& d = host_descs_[(size_t)s];
         // Reconstruction: tiles holding band cells store the strips forward; the
@@ -688,7 +727,8 @@ int Engine::build_tiles() {
         };
         for (int tz = 0; tz < j.gs.ntz; ++tz)
             for (int tx = 0; tx < ntx; ++tx) {
-                TileRef r = place_vd(make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0, nbuf_));
+                TileRef r = place_vd(make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0, nbuf_,
+                                                   false, j.gs.z0));
                 if (rec && (meets(tx, tz, nb - H, nb, nb, nb + j.gs.nz) ||
                             meets(tx, tz, nb + j.gs.nx, nb + j.gs.nx + H, nb, nb + j.gs.nz) ||
                             meets(tx, tz, nb, nb + j.gs.nx, nb - H, nb) ||
@@ -705,6 +745,7 @@ int Engine::build_tiles() {
         sig.push_back(j.m->half);
         sig.push_back(ntx);
         sig.push_back(j.gs.ntz);
+        sig.push_back(j.gs.z0);
         sig.push_back(j.g0);
         sig.push_back(j.total);
         sig.push_back(d.flags);
@@ -835,7 +876,7 @@ int Engine::run_chunk(int steps) {
             std::vector<TuneChoice> cands = {{kStepRing, 4, 16, 0, 3, 0}, {kStepRing, 4, 16, 0, 3, 1},
                                              {kStepRing, 8, 16, 0, 3, 0}, {kStepRing, 8, 16, 0, 3, 1},
                                              {kStepRing, 8, 32, 0, 3, 0}};
-            if (exact())
+            if (exact() && !shifted_bands())
                 for (int m : {2, 3, 5}) cands.push_back({kStepMarch, 8, 16, 0, m, 0});
             if (pin_kind_ >= 0) {
                 std::vector<TuneChoice> keep;

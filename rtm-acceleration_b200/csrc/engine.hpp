@@ -204,6 +204,8 @@ private:
     int shared_vd_buf() const { return nslots_ * nbuf_; }
     int pool_buffers() const { return nslots_ * nbuf_ + (f64_ ? 0 : 1); }
     int share_model_vdt2(const Model* m);
+    bool shifted_bands() const;   // an active job's bands start at a row other than 0
+    bool band_shift_ = true;      // FMA ring jobs may start their bands at row H & ~3
     struct MapPair { CUtensorMap pc, box; };
     std::map<int, MapPair> maps_;            // by (half, tile width): p^n box with halo; 128 x TX box
     std::vector<Slot> slots_;

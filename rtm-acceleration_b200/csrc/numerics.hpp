@@ -58,7 +58,9 @@ struct GridDims {
     int ldz = 0;      // field column pitch: nze rounded up to 8 (32-byte columns)
     int zs0 = 0;      // first stored row of snapshots/images: nb rounded down to 4
     int lds = 0;      // stored rows: [zs0, round_up4(nb+nz))
-    int ntz = 0;      // 128-row tiles covering nze
+    int ntz = 0;      // 128-row tiles covering nze (from row z0)
+    int z0 = 0;       // first row of the 128-row bands; rows above them and below
+                      // the last one belong to the zero ring (engine jobs only)
 };
 GridDims make_grid(int nx, int nz, int nb, int half);
 

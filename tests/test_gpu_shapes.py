@@ -67,3 +67,24 @@ def test_batch_shapes_agree_bitwise(ring_only, snap, acc):
     tol = 1e-5 if snap == "f32" else 1e-3
     assert rel_l2(ref64, out[0][0]) <= tol
     assert rel_l2(ill64, out[0][1]) <= tol
+
+
+@pytest.mark.parametrize("snap", ["f32", "bf16"])
+def test_batch_band_origin_shift_bitwise(monkeypatch, snap):
+    """nze = 264 = 2 x 128 + 8 at order 8: the batch (FMA) engine starts its
+    128-row bands at row 4, so two bands cover the live rows 4-259 where bands
+    from row 0 need a third of 8 rows.  Same cells, so the images agree bit for
+    bit with RTM_B200_BAND_SHIFT=0, and with the FP64 oracle within the
+    tolerances above."""
+    p, v, shots = small_problem(order=8, nx=90, nz=164, nb=50, nt=220, nshots=3, si=2)
+    out = []
+    for shift in ("1", "0"):
+        monkeypatch.setenv("RTM_B200_BAND_SHIFT", shift)
+        with make_engine("batch", p, v, snap=snap, max_shots_in_flight=3) as e:
+            out.append(e.migrate(shots))
+    for a, b in zip(out[0], out[1]):
+        assert bits_equal(a, b), rel_l2(a, b)
+    ref64, ill64 = oracle.migrate(p, v, shots, np.float64)
+    tol = 1e-5 if snap == "f32" else 1e-3
+    assert rel_l2(ref64, out[0][0]) <= tol
+    assert rel_l2(ill64, out[0][1]) <= tol
