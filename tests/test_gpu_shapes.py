@@ -70,13 +70,15 @@ def test_batch_shapes_agree_bitwise(ring_only, snap, acc):
 
 
 @pytest.mark.parametrize("snap", ["f32", "bf16"])
-def test_batch_band_origin_shift_bitwise(monkeypatch, snap):
-    """nze = 264 = 2 x 128 + 8 at order 8: the batch (FMA) engine starts its
-    128-row bands at row 4, so two bands cover the live rows 4-259 where bands
-    from row 0 need a third of 8 rows.  Same cells, so the images agree bit for
-    bit with RTM_B200_BAND_SHIFT=0, and with the FP64 oracle within the
-    tolerances above."""
-    p, v, shots = small_problem(order=8, nx=90, nz=164, nb=50, nt=220, nshots=3, si=2)
+@pytest.mark.parametrize("order", [8, 12])
+def test_batch_band_origin_shift_bitwise(monkeypatch, snap, order):
+    """nze = 264 = 2 x 128 + 8: the batch (FMA) engine starts its 128-row bands
+    at row 4, so two bands cover the live rows (4-259 at order 8, 6-257 at
+    order 12, whose first p^n box then starts at row -4) where bands from row 0
+    need a third.  Same cells, so the images agree bit for bit with
+    RTM_B200_BAND_SHIFT=0, and with the FP64 oracle within the tolerances
+    above."""
+    p, v, shots = small_problem(order=order, nx=90, nz=164, nb=50, nt=220, nshots=3, si=2)
     out = []
     for shift in ("1", "0"):
         monkeypatch.setenv("RTM_B200_BAND_SHIFT", shift)
