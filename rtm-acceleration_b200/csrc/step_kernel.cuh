@@ -532,9 +532,15 @@ __device__ __forceinline__ void column_epilogue(const ShotDesc& d, const TileInf
         if (col_int && lane_snap)
 #pragma unroll
             for (int q = 0; q < 4; ++q) a = fmaxf(a, fabsf((float)val[q]));
+        if (G == 32) {
+            // one warp-wide reduction: for non-negative floats the order of
+            // the bit patterns as unsigned integers is the order of the values
+            a = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(a)));
+        } else {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-            if (o < G) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+            for (int o = 16; o > 0; o >>= 1)
+                if (o < G) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+        }
         amax_col = a;
     }
 
