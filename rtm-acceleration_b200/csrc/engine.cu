@@ -141,8 +141,9 @@ int Engine::init() {
     // column-pair shapes.
     if (const char* w = std::getenv("RTM_B200_RING_WARPS"))
         if (tile_x_ == 16 && cfg_.tile_cols != 0 && std::atoi(w) == 8) warps_ = 8;
-    // Test hook: RTM_B200_BAND_SHIFT=0 keeps every job's bands at row 0, so tests
-    // can compare shifted and unshifted band origins bit for bit.
+    // Test hook: RTM_B200_BAND_SHIFT=0 keeps every job's bands at row 0 and tile
+    // columns at column 0, so tests can compare shifted and unshifted tilings
+    // bit for bit.
     if (const char* b = std::getenv("RTM_B200_BAND_SHIFT")) band_shift_ = std::atoi(b) != 0;
     autotune_ = cfg_.tile_cols == 0;
     // Failure-detection test hook: the first step launch leaves this tile's
@@ -442,10 +443,15 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
     {
         const int H = m->half, s0 = H & ~3;
         const int ntz_s = (job.gs.nze - H - s0 + kTileZ - 1) / kTileZ;
-        if (band_shift_ && !modelling && !recon_ && !exact() && s0 > 0 && job.gs.nb >= s0 && ntz_s < job.gs.ntz) {
+        const bool shiftable = band_shift_ && !modelling && !recon_ && !exact();
+        if (shiftable && s0 > 0 && job.gs.nb >= s0 && ntz_s < job.gs.ntz) {
             job.gs.z0 = s0;
             job.gs.ntz = ntz_s;
         }
+        // Columns likewise: the tile columns may start at column H (the column
+        // coordinate of a TMA box has no alignment rule), which saves a tile
+        // column whenever the live columns [H, nxe - H) fit in one fewer.
+        job.shift_cols = shiftable && job.gs.nb >= H;
     }
     job.x0 = sh.x0;
     job.modelling = modelling;
@@ -612,6 +618,18 @@ int Engine::start_job(int s, Model* m, int shot, bool modelling, float* rec_host
                                 sizeof(ShotDesc));
     RTMB_CUDA(cudaMemcpyAsync(descs_.get<ShotDesc>() + s, st + o_desc, sizeof(ShotDesc), cudaMemcpyHostToDevice,
                               stream_));
+    // Columns [0, H) and [nxe - H, nxe_cap) of a job whose tile columns may
+    // start at H: zero in both field levels (tiles need not cover them).
+    if (job.shift_cols) {
+        const size_t col = (size_t)ldz_cap_ * elem();
+        const int H = m->half;
+        for (int b = 0; b < 2; ++b) {
+            char* fb = pool_.get<char>() + ((size_t)s * nbuf_ + b) * nxe_cap_ * ldz_cap_ * elem();
+            RTMB_CUDA(cudaMemsetAsync(fb, 0, (size_t)H * col, stream_));
+            RTMB_CUDA(cudaMemsetAsync(fb + (size_t)(gs.nxe - H) * col, 0, (size_t)(nxe_cap_ - gs.nxe + H) * col,
+                                      stream_));
+        }
+    }
     // Rows outside a shifted job's bands: zero in both field levels.
     if (gs.z0 > 0) {
         const size_t pitch = (size_t)ldz_cap_ * elem();
@@ -702,10 +720,13 @@ int Engine::build_tiles() {
         const Job& j = jobs_[(size_t)s];
         if (!j.active) continue;
         const int TX = step_tile_x(variant(j.m->half));
-        const int ntx = (j.gs.nxe + TX - 1) / TX;
+        const int H0 = j.m->half;
+        const int ntx0 = (j.gs.nxe + TX - 1) / TX, ntx1 = (j.gs.nxe - 2 * H0 + TX - 1) / TX;
+        const int cx0 = j.shift_cols && ntx1 < ntx0 ? H0 : 0;   // first column of the tile columns
+        const int ntx = cx0 ? ntx1 : ntx0;
         std::vector<uint8_t> tflags((size_t)ntx * j.gs.ntz, 0);
         for (const auto& c : j.rec_cells)
-            tflags[(size_t)(c.first / TX) * j.gs.ntz + (c.second - j.gs.z0) / kTileZ] = 1;
+            tflags[(size_t)((c.first - cx0) / TX) * j.gs.ntz + (c.second - j.gs.z0) / kTileZ] = 1;
         auto& vec = by_half[j.m->half];
         const ShotDesc& d = host_descs_[(size_t)s];
         // Reconstruction: tiles holding band cells store the strips forward; the
@@ -728,7 +749,7 @@ int Engine::build_tiles() {
         for (int tz = 0; tz < j.gs.ntz; ++tz)
             for (int tx = 0; tx < ntx; ++tx) {
                 TileRef r = place_vd(make_tile_ref(d, s, tx, tz, TX, tflags[(size_t)tx * j.gs.ntz + tz] != 0, nbuf_,
-                                                   false, j.gs.z0));
+                                                   false, j.gs.z0, cx0));
                 if (rec && (meets(tx, tz, nb - H, nb, nb, nb + j.gs.nz) ||
                             meets(tx, tz, nb + j.gs.nx, nb + j.gs.nx + H, nb, nb + j.gs.nz) ||
                             meets(tx, tz, nb, nb + j.gs.nx, nb - H, nb) ||
@@ -746,6 +767,7 @@ int Engine::build_tiles() {
         sig.push_back(ntx);
         sig.push_back(j.gs.ntz);
         sig.push_back(j.gs.z0);
+        sig.push_back(cx0);
         sig.push_back(j.g0);
         sig.push_back(j.total);
         sig.push_back(d.flags);

@@ -85,6 +85,8 @@ struct Job {
     int total = 0;                     // steps: nt (modelling) or 2 nt
     int first_phase_step = 0;          // 0, or nt for a backward-only job
     bool modelling = false;
+    bool shift_cols = false;           // tiles may start at column H (FMA ring jobs; columns
+                                       // [0, H) and [nxe - H, ..) are cleared at set-up)
     float* rec_host = nullptr;
     size_t snap_off = 0, snap_bytes = 0;
     bool owns_snap = false;

@@ -159,11 +159,12 @@ static_assert(sizeof(TileRef) == 80, "TileRef layout");
 
 // Host-side construction of a TileRef from the slot's descriptor.
 inline TileRef make_tile_ref(const ShotDesc& d, int slot, int tx, int tz, int tile_x, bool has_pts,
-                             int nbuf = kFieldBuffers, bool source_tile = false, int band_z0 = 0) {
+                             int nbuf = kFieldBuffers, bool source_tile = false, int band_z0 = 0,
+                             int band_x0 = 0) {
     TileRef r{};
     r.slot = slot;
     r.has_pts = has_pts ? 1 : 0;
-    r.x0 = tx * tile_x;
+    r.x0 = band_x0 + tx * tile_x;
     r.z0 = band_z0 + tz * kTileZ;
     r.field_base = d.field_slot * nbuf;
     r.vd_x = r.x0;

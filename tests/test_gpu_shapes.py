@@ -75,10 +75,11 @@ def test_batch_band_origin_shift_bitwise(monkeypatch, snap, order):
     """nze = 264 = 2 x 128 + 8: the batch (FMA) engine starts its 128-row bands
     at row 4, so two bands cover the live rows (4-259 at order 8, 6-257 at
     order 12, whose first p^n box then starts at row -4) where bands from row 0
-    need a third.  Same cells, so the images agree bit for bit with
-    RTM_B200_BAND_SHIFT=0, and with the FP64 oracle within the tolerances
-    above."""
-    p, v, shots = small_problem(order=order, nx=90, nz=164, nb=50, nt=220, nshots=3, si=2)
+    need a third; nxe = 184 = 11 x 16 + 8: its 16-column tiles start at column
+    H, so 11 tile columns cover the live columns where 12 start at column 0.
+    Same cells, so the images agree bit for bit with RTM_B200_BAND_SHIFT=0, and
+    with the FP64 oracle within the tolerances above."""
+    p, v, shots = small_problem(order=order, nx=84, nz=164, nb=50, nt=220, nshots=3, si=2)
     out = []
     for shift in ("1", "0"):
         monkeypatch.setenv("RTM_B200_BAND_SHIFT", shift)
